@@ -1,0 +1,177 @@
+"""ctypes view of the C ABI in include/falconnpp_b200.h.
+
+Used by the tests and the benchmark to call the library exactly as a foreign
+caller (cgo, JNI, another C program) would: plain pointers and sizes.
+``Index`` wraps one handle and raises ``FppError`` on a negative status.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from . import LIBRARY_PATH, _require_native
+
+# Every symbol the header declares (tests check the library exports them all).
+EXPORTED = [
+    "fpp_create", "fpp_destroy", "fpp_set_index_param", "fpp_set_qprobes", "fpp_set_threads", "fpp_clear",
+    "fpp_build", "fpp_build_device", "fpp_query", "fpp_query_device", "fpp_last_error", "fpp_get_info",
+    "fpp_get_stats", "fpp_set_option", "fpp_print_build_report", "fpp_dump_bits", "fpp_dump_center",
+    "fpp_dump_tables", "fpp_build_dump_hash", "fpp_query_dump",
+]
+
+_lib = None
+
+
+class FppError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        _require_native()
+        L = ctypes.CDLL(LIBRARY_PATH)
+        vp, i32, i64, f32 = ctypes.c_void_p, ctypes.c_int, ctypes.c_longlong, ctypes.c_float
+        sig = {
+            "fpp_create": (i32, [i32, i32, ctypes.POINTER(vp)]),
+            "fpp_destroy": (None, [vp]),
+            "fpp_set_index_param": (i32, [vp, i32, i32, i32, f32, i32, i32, i32]),
+            "fpp_set_qprobes": (i32, [vp, i32]),
+            "fpp_set_threads": (i32, [vp, i32]),
+            "fpp_clear": (i32, [vp]),
+            "fpp_build": (i32, [vp, vp]),
+            "fpp_build_device": (i32, [vp, vp, vp]),
+            "fpp_query": (i32, [vp, vp, i32, i32, i32, vp]),
+            "fpp_query_device": (i32, [vp, vp, i32, i32, vp, vp]),
+            "fpp_last_error": (ctypes.c_char_p, []),
+            "fpp_get_info": (i32, [vp, vp, i32]),
+            "fpp_get_stats": (i32, [vp, i32, vp, i32]),
+            "fpp_set_option": (i32, [vp, ctypes.c_char_p, i64]),
+            "fpp_print_build_report": (None, [vp]),
+            "fpp_dump_bits": (i32, [vp, vp, vp]),
+            "fpp_dump_center": (i32, [vp, vp]),
+            "fpp_dump_tables": (i32, [vp, vp, vp]),
+            "fpp_build_dump_hash": (i32, [vp, vp, vp, vp]),
+            "fpp_query_dump": (i32, [vp, vp, i32, i32, vp, vp, vp, vp, vp, vp, i64]),
+        }
+        for name, (res, args) in sig.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _check(rc: int) -> None:
+    if rc != 0:
+        raise FppError(rc, lib().fpp_last_error().decode())
+
+
+def _ptr(a: np.ndarray | None):
+    return None if a is None else a.ctypes.data
+
+
+class Index:
+    """One index handle.  Points/queries are (n, d) float32 C-contiguous arrays
+    (the memory layout of the reference's d x n column-major matrices)."""
+
+    def __init__(self, n_points: int, n_features: int):
+        self.n, self.d = n_points, n_features
+        h = ctypes.c_void_p()
+        _check(lib().fpp_create(n_points, n_features, ctypes.byref(h)))
+        self.h = h
+
+    def close(self):
+        if self.h:
+            lib().fpp_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_index_param(self, n_tables, n_proj, bucket_minSize, bucket_scale, iProbes, n_threads=8, random_seed=-1):
+        _check(lib().fpp_set_index_param(self.h, n_tables, n_proj, bucket_minSize, bucket_scale, iProbes, n_threads,
+                                         random_seed))
+        self.L, self.D, self.iProbes = n_tables, n_proj, iProbes
+
+    def set_qprobes(self, q: int):
+        _check(lib().fpp_set_qprobes(self.h, q))
+
+    def set_option(self, key: str, value: int):
+        _check(lib().fpp_set_option(self.h, key.encode(), int(value)))
+
+    def build(self, X: np.ndarray):
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        assert X.shape == (self.n, self.d)
+        _check(lib().fpp_build(self.h, _ptr(X)))
+
+    def build_device(self, ptr: int, stream: int | None = None):
+        _check(lib().fpp_build_device(self.h, ctypes.c_void_p(ptr), ctypes.c_void_p(stream or 0)))
+
+    def build_dump_hash(self, X: np.ndarray):
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        codes = np.zeros((self.L, self.n, self.iProbes), np.int32)
+        scores = np.zeros((self.L, self.n, self.iProbes), np.float32)
+        _check(lib().fpp_build_dump_hash(self.h, _ptr(X), _ptr(codes), _ptr(scores)))
+        return codes, scores
+
+    def query(self, Q: np.ndarray, k: int, verbose: bool = False) -> np.ndarray:
+        Q = np.ascontiguousarray(Q, dtype=np.float32)
+        out = np.zeros((Q.shape[0], k), np.int32)
+        _check(lib().fpp_query(self.h, _ptr(Q), Q.shape[0], k, int(verbose), _ptr(out)))
+        return out
+
+    def query_device(self, q_ptr: int, nq: int, k: int, out_ptr: int, stream: int | None = None):
+        _check(lib().fpp_query_device(self.h, ctypes.c_void_p(q_ptr), nq, k, ctypes.c_void_p(out_ptr),
+                                      ctypes.c_void_p(stream or 0)))
+
+    def query_dump(self, Q: np.ndarray, k: int, qprobes: int, cand_cap: int = 0):
+        Q = np.ascontiguousarray(Q, dtype=np.float32)
+        nq = Q.shape[0]
+        out = np.zeros((nq, k), np.int32)
+        val = np.zeros((nq, k), np.float32)
+        probes = np.zeros((nq, qprobes), np.uint32)
+        pval = np.zeros((nq, qprobes), np.float32)
+        stats = np.zeros((nq, 4), np.int64)
+        cands = np.full((nq, cand_cap), -1, np.int32) if cand_cap else None
+        _check(lib().fpp_query_dump(self.h, _ptr(Q), nq, k, _ptr(out), _ptr(val), _ptr(probes), _ptr(pval),
+                                    _ptr(stats), _ptr(cands), cand_cap))
+        return dict(topk=out, topk_val=val, probes=probes, probe_val=pval, stats=stats, cands=cands)
+
+    def info(self) -> dict:
+        v = np.zeros(6, np.int64)
+        _check(lib().fpp_get_info(self.h, _ptr(v), 6))
+        return dict(fhtDim=int(v[0]), n_ids=int(v[1]), max_kept=int(v[2]), n_buckets=int(v[3]), built=bool(v[4]),
+                    device=int(v[5]))
+
+    def stats(self, kind: int) -> np.ndarray:
+        v = np.zeros(8, np.float64)
+        _check(lib().fpp_get_stats(self.h, kind, _ptr(v), 8))
+        return v
+
+    def dump_bits(self):
+        info = self.info()
+        nbits = self.L * 3 * info["fhtDim"]
+        b1 = np.zeros(nbits, np.uint8)
+        b2 = np.zeros(nbits, np.uint8)
+        _check(lib().fpp_dump_bits(self.h, _ptr(b1), _ptr(b2)))
+        return b1, b2
+
+    def dump_center(self):
+        c = np.zeros(self.d, np.float32)
+        _check(lib().fpp_dump_center(self.h, _ptr(c)))
+        return c
+
+    def dump_tables(self):
+        info = self.info()
+        start = np.zeros(info["n_buckets"] + 1, np.uint32)
+        ids = np.zeros(max(1, info["n_ids"]), np.int32)
+        _check(lib().fpp_dump_tables(self.h, _ptr(start), _ptr(ids)))
+        return start, ids[: info["n_ids"]]

@@ -1,0 +1,447 @@
+// fpp_capi.cu — the extern "C" boundary (include/falconnpp_b200.h) over the
+// device index: parameter handling as in FalconnPP::Index2Layers
+// (src/FalconnPP.h:85-123), the random signs of bitHD3Generator2
+// (src/FalconnPP.h:52-75, same libstdc++ engine and distribution), status
+// codes instead of undefined behaviour, and the verbose side effects of
+// query2Layers_1D (src/FalconnPP.cpp:682-703).
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <chrono>
+#include <fstream>
+#include <iostream>
+#include <mutex>
+#include <random>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "../../include/falconnpp_b200.h"
+#include "fpp_index.h"
+#include "fpp_query.h"
+
+struct fpp_index {
+  fpp::Params P;
+  fpp::DeviceIndex di;
+  fpp::QueryWorkspace ws;
+  fpp::HostBits bits;
+  fpp::BuildOptions opt;
+  fpp::BuildStats bst;
+  fpp::QueryStats qst;
+  bool params_set = false;
+  bool built = false;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::mutex mu;
+};
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+int ok() {
+  g_last_error.clear();
+  return FPP_OK;
+}
+
+bool is_pow2(int x) { return x > 0 && (x & (x - 1)) == 0; }
+
+// src/FalconnPP.h:52-68: one default_random_engine, two draws per position.
+void generate_bits(const fpp::Params& P, fpp::HostBits& b) {
+  const int nbits = P.fhtDim * P.n_tables * P.n_rotate;
+  unsigned seed = std::chrono::system_clock::now().time_since_epoch().count();
+  if (P.seed > -1) seed = (unsigned)P.seed;
+  std::default_random_engine generator(seed);
+  std::uniform_int_distribution<uint32_t> unifDist(0, 1);
+  b.b1.assign(nbits, 0);
+  b.b2.assign(nbits, 0);
+  for (int d = 0; d < nbits; ++d) {
+    b.b1[d] = unifDist(generator) & 1;
+    b.b2[d] = unifDist(generator) & 1;
+  }
+}
+
+int use_device(fpp_index* h) {
+  cudaError_t e = cudaSetDevice(h->device);
+  if (e != cudaSuccess) return fail(FPP_ERR_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
+  return FPP_OK;
+}
+
+int check_query_params(const fpp_index* h, int n_queries, int k) {
+  if (!h->built) return fail(FPP_ERR_NOT_BUILT, "query: the index is not built");
+  if (n_queries < 0) return fail(FPP_ERR_INVALID_ARGUMENT, "query: n_queries must be >= 0");
+  if (k < 1 || k > 1024) return fail(FPP_ERR_INVALID_ARGUMENT, "query: n_neighbors must be in [1, 1024]");
+  const fpp::Params& P = h->P;
+  if (P.qProbes < 1) return fail(FPP_ERR_INVALID_ARGUMENT, "query: qProbes must be >= 1");
+  const int m = (int)ceil(2.0 * P.qProbes / P.n_tables);
+  const int m1 = (int)ceil(sqrt(1.0 * m));
+  if (m1 > P.n_proj || m1 > 64)
+    return fail(FPP_ERR_INVALID_ARGUMENT,
+                "query: qProbes too large: ceil(sqrt(ceil(2*qProbes/n_tables))) must be <= min(n_proj, 64)");
+  if ((long long)P.n_tables * m > (1LL << 24))
+    return fail(FPP_ERR_INVALID_ARGUMENT, "query: n_tables * probes per table too large");
+  return FPP_OK;
+}
+
+std::string int2str(int x) {
+  std::stringstream ss;
+  ss << x;
+  return ss.str();
+}
+
+int do_build(fpp_index* h, const float* X, bool on_device, cudaStream_t s, int32_t* codes_host, float* scores_host) {
+  if (!h->params_set) return fail(FPP_ERR_INVALID_ARGUMENT, "build: call setIndexParam first");
+  if (!X) return fail(FPP_ERR_INVALID_ARGUMENT, "build: dataset is NULL");
+  if (use_device(h)) return FPP_ERR_CUDA;
+  fpp::Params& P = h->P;
+  generate_bits(P, h->bits);
+  int32_t* dcodes = nullptr;
+  float* dscores = nullptr;
+  const size_t ncodes = (size_t)P.n_tables * P.n_points * P.iProbes;
+  if (codes_host) {
+    if (cudaMalloc(&dcodes, sizeof(int32_t) * ncodes) != cudaSuccess ||
+        cudaMalloc(&dscores, sizeof(float) * ncodes) != cudaSuccess) {
+      cudaFree(dcodes);
+      return fail(FPP_ERR_OUT_OF_MEMORY, "build: cannot allocate the hash-code dump");
+    }
+  }
+  h->ws.release();
+  h->built = false;
+  fpp::Error err{0, ""};
+  h->bst = fpp::BuildStats();
+  const int rc = fpp::build_index(P, X, on_device, h->bits, h->opt, h->di, h->bst, s, err, dcodes, dscores);
+  if (rc == FPP_OK && codes_host) {
+    cudaMemcpy(codes_host, dcodes, sizeof(int32_t) * ncodes, cudaMemcpyDeviceToHost);
+    cudaMemcpy(scores_host, dscores, sizeof(float) * ncodes, cudaMemcpyDeviceToHost);
+  }
+  cudaFree(dcodes);
+  cudaFree(dscores);
+  if (rc != FPP_OK) return fail(rc, err.msg);
+  h->built = true;
+  return ok();
+}
+
+void print_build(const fpp_index* h) {
+  // src/FalconnPP.cpp:23-30 and :281-301
+  const fpp::Params& P = h->P;
+  std::cout << "n_points: " << P.n_points << std::endl;
+  std::cout << "n_features: " << P.n_features << std::endl;
+  std::cout << "n_tables: " << P.n_tables << std::endl;
+  std::cout << "n_proj: " << P.n_proj << std::endl;
+  std::cout << "fhtDim: " << P.fhtDim << std::endl;
+  std::cout << "# iProbes: " << P.iProbes << std::endl;
+  std::cout << "bucket_minSize: " << P.bucket_minSize << std::endl;
+  std::cout << "bucket_scale: " << P.bucket_scale << std::endl;
+  std::cout << "Finish building index... " << std::endl;
+  const double nb = 4.0 * P.n_proj * P.n_proj * P.n_tables;
+  const double size_1d = 1.0 * sizeof(int32_t) * h->di.n_ids / (1 << 30);
+  const double size_pos = 1.0 * sizeof(uint32_t) * (nb + 1) / (1 << 30);
+  std::cout << "Size of vecTables_1D in GB: " << size_1d << std::endl;
+  std::cout << "Size of vecPair_BucketPos in GB: " << size_pos << std::endl;
+  std::cout << "Size of Falconn++ (2 layers) index in GB: " << size_1d + size_pos << std::endl;
+  std::cout << "n_points per table / n: " << h->bst.points_per_table << std::endl;
+  std::cout << "Percentage of scaled buckets in a table: " << 1.0 * h->bst.n_limited / nb << std::endl;
+  std::cout << "Construct Falconn++ (2 layers) Wall Time (in seconds): " << (float)(int)(h->bst.ms_total / 1000.0)
+            << " seconds" << std::endl;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* fpp_last_error(void) { return g_last_error.c_str(); }
+
+int fpp_create(int n_points, int n_features, fpp_index** out) {
+  if (!out) return fail(FPP_ERR_INVALID_ARGUMENT, "create: out is NULL");
+  *out = nullptr;
+  if (n_points < 1) return fail(FPP_ERR_INVALID_ARGUMENT, "create: n_points must be >= 1");
+  if (n_features < 1) return fail(FPP_ERR_INVALID_ARGUMENT, "create: n_features must be >= 1");
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return fail(FPP_ERR_DEVICE, std::string("create: no CUDA device: ") + cudaGetErrorString(e));
+  fpp_index* h = new fpp_index();
+  h->P.n_points = n_points;
+  h->P.n_features = n_features;
+  h->device = dev;
+  e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    delete h;
+    return fail(FPP_ERR_CUDA, std::string("create: cudaStreamCreate: ") + cudaGetErrorString(e));
+  }
+  *out = h;
+  return ok();
+}
+
+void fpp_destroy(fpp_index* h) {
+  if (!h) return;
+  {
+    std::lock_guard<std::mutex> g(h->mu);
+    cudaSetDevice(h->device);
+    h->ws.release();
+    fpp::free_index(h->di);
+    if (h->stream) cudaStreamDestroy(h->stream);
+  }
+  delete h;
+}
+
+int fpp_set_index_param(fpp_index* h, int n_tables, int n_proj, int bucket_minSize, float bucket_scale,
+                        int iProbes, int n_threads, int random_seed) {
+  if (!h) return fail(FPP_ERR_INVALID_ARGUMENT, "setIndexParam: NULL handle");
+  std::lock_guard<std::mutex> g(h->mu);
+  if (n_tables < 1) return fail(FPP_ERR_INVALID_ARGUMENT, "setIndexParam: n_tables must be >= 1");
+  if (!is_pow2(n_proj)) return fail(FPP_ERR_INVALID_ARGUMENT, "setIndexParam: n_proj must be a power of two");
+  const int fht = fpp::derived_fht_dim(h->P.n_features, n_proj);
+  if (fht > 1024 || n_proj > 1024)
+    return fail(FPP_ERR_UNSUPPORTED, "setIndexParam: fhtDim = 2^ceil(log2(max(d, n_proj))) must be <= 1024");
+  if (fht < 2) return fail(FPP_ERR_UNSUPPORTED, "setIndexParam: fhtDim must be >= 2");
+  if (iProbes < 1 || iProbes > 32 || iProbes > n_proj)
+    return fail(FPP_ERR_INVALID_ARGUMENT, "setIndexParam: iProbes must be in [1, min(32, n_proj)]");
+  if (!(bucket_scale >= 0.0f) || !isfinite(bucket_scale))
+    return fail(FPP_ERR_INVALID_ARGUMENT, "setIndexParam: bucket_scale must be finite and >= 0");
+  if ((long long)n_tables * 4LL * n_proj * n_proj >= (1LL << 31))
+    return fail(FPP_ERR_UNSUPPORTED, "setIndexParam: n_tables * 4 * n_proj^2 must be < 2^31 (int bucket ids)");
+  fpp::Params& P = h->P;
+  P.n_tables = n_tables;
+  P.n_proj = n_proj;
+  P.bucket_minSize = bucket_minSize;
+  P.bucket_scale = bucket_scale;
+  P.iProbes = iProbes;
+  P.n_threads = n_threads;
+  P.seed = random_seed;
+  P.fhtDim = fht;
+  h->params_set = true;
+  return ok();
+}
+
+int fpp_set_qprobes(fpp_index* h, int qProbes) {
+  if (!h) return fail(FPP_ERR_INVALID_ARGUMENT, "set_qProbes: NULL handle");
+  if (qProbes < 1) return fail(FPP_ERR_INVALID_ARGUMENT, "set_qProbes: qProbes must be >= 1");
+  std::lock_guard<std::mutex> g(h->mu);
+  h->P.qProbes = qProbes;
+  return ok();
+}
+
+int fpp_set_threads(fpp_index* h, int n_threads) {
+  if (!h) return fail(FPP_ERR_INVALID_ARGUMENT, "set_threads: NULL handle");
+  std::lock_guard<std::mutex> g(h->mu);
+  h->P.n_threads = n_threads;
+  return ok();
+}
+
+int fpp_clear(fpp_index* h) {
+  if (!h) return fail(FPP_ERR_INVALID_ARGUMENT, "clear: NULL handle");
+  std::lock_guard<std::mutex> g(h->mu);
+  cudaSetDevice(h->device);
+  h->ws.release();
+  fpp::free_index(h->di);
+  h->bits = fpp::HostBits();
+  h->built = false;
+  return ok();
+}
+
+int fpp_set_option(fpp_index* h, const char* key, long long value) {
+  if (!h || !key) return fail(FPP_ERR_INVALID_ARGUMENT, "set_option: NULL argument");
+  std::lock_guard<std::mutex> g(h->mu);
+  if (!strcmp(key, "exact_bucket_order")) {
+    h->opt.exact_bucket_order = value != 0;
+  } else if (!strcmp(key, "tables_per_chunk")) {
+    if (value < 0) return fail(FPP_ERR_INVALID_ARGUMENT, "set_option: tables_per_chunk must be >= 0");
+    h->opt.tables_per_chunk = (int)value;
+  } else {
+    return fail(FPP_ERR_INVALID_ARGUMENT, std::string("set_option: unknown key ") + key);
+  }
+  return ok();
+}
+
+int fpp_build(fpp_index* h, const float* dataset) {
+  if (!h) return fail(FPP_ERR_INVALID_ARGUMENT, "build: NULL handle");
+  std::lock_guard<std::mutex> g(h->mu);
+  const int rc = do_build(h, dataset, false, h->stream, nullptr, nullptr);
+  return rc;
+}
+
+int fpp_build_device(fpp_index* h, const float* d_dataset, void* stream) {
+  if (!h) return fail(FPP_ERR_INVALID_ARGUMENT, "build: NULL handle");
+  std::lock_guard<std::mutex> g(h->mu);
+  cudaStream_t s = stream ? (cudaStream_t)stream : h->stream;
+  return do_build(h, d_dataset, true, s, nullptr, nullptr);
+}
+
+int fpp_build_dump_hash(fpp_index* h, const float* dataset, int32_t* codes, float* scores) {
+  if (!h || !codes || !scores) return fail(FPP_ERR_INVALID_ARGUMENT, "build_dump_hash: NULL argument");
+  std::lock_guard<std::mutex> g(h->mu);
+  return do_build(h, dataset, false, h->stream, codes, scores);
+}
+
+int fpp_query(fpp_index* h, const float* queries, int n_queries, int n_neighbors, int verbose, int32_t* out) {
+  if (!h) return fail(FPP_ERR_INVALID_ARGUMENT, "query: NULL handle");
+  std::lock_guard<std::mutex> g(h->mu);
+  int rc = check_query_params(h, n_queries, n_neighbors);
+  if (rc) return rc;
+  if (n_queries > 0 && (!queries || !out)) return fail(FPP_ERR_INVALID_ARGUMENT, "query: NULL buffer");
+  if (use_device(h)) return FPP_ERR_CUDA;
+  const fpp::Params& P = h->P;
+  if (verbose) {
+    std::cout << "number of queries: " << n_queries << std::endl;
+    std::cout << "# qProbes: " << P.qProbes << std::endl;
+    std::cout << "number of threads: " << P.n_threads << std::endl;
+  }
+  const auto t0 = std::chrono::high_resolution_clock::now();
+  fpp::Error err{0, ""};
+  rc = fpp::query_index(P, h->di, queries, false, n_queries, n_neighbors, out, false, h->ws, h->qst, h->stream, err,
+                        nullptr);
+  if (rc) return fail(rc, err.msg);
+  if (verbose && n_queries > 0) {
+    const auto ms = std::chrono::duration_cast<std::chrono::milliseconds>(std::chrono::high_resolution_clock::now() - t0);
+    const fpp::QueryStats& s = h->qst;
+    std::cout << "Average number of empty buckets per query: " << (float)s.total_empty / n_queries << std::endl;
+    std::cout << "Average number of probes per query: " << (float)s.total_probes / n_queries << std::endl;
+    std::cout << "Average number of unique candidates per query: " << (float)s.total_unique / n_queries << std::endl;
+    std::cout << "Average number of candidates per query: " << (float)s.total_cand / n_queries << std::endl;
+    std::cout << "Querying Time: " << (float)ms.count() << " ms" << std::endl;
+    const std::string fn = "1D_Top_" + int2str(n_neighbors) + "_D_" + int2str(P.n_proj) + "_L_" +
+                           int2str(P.n_tables) + "_iProbe_" + int2str(P.iProbes) + "_bucketMinSize_" +
+                           int2str(P.bucket_minSize) + "_bucketScale_" + int2str((int)(P.bucket_scale * 100)) +
+                           "_qProbe_" + int2str(P.qProbes) + ".txt";
+    std::ofstream f(fn);  // src/Utilities.cpp:13-33: one query per line
+    for (int q = 0; q < n_queries; ++q) {
+      for (int j = 0; j < n_neighbors; ++j) f << out[(size_t)q * n_neighbors + j] << ' ';
+      f << '\n';
+    }
+  }
+  return ok();
+}
+
+int fpp_query_device(fpp_index* h, const float* d_queries, int n_queries, int n_neighbors, int32_t* d_out,
+                     void* stream) {
+  if (!h) return fail(FPP_ERR_INVALID_ARGUMENT, "query: NULL handle");
+  std::lock_guard<std::mutex> g(h->mu);
+  int rc = check_query_params(h, n_queries, n_neighbors);
+  if (rc) return rc;
+  if (n_queries > 0 && (!d_queries || !d_out)) return fail(FPP_ERR_INVALID_ARGUMENT, "query: NULL buffer");
+  if (use_device(h)) return FPP_ERR_CUDA;
+  cudaStream_t s = stream ? (cudaStream_t)stream : h->stream;
+  fpp::Error err{0, ""};
+  rc = fpp::query_index(h->P, h->di, d_queries, true, n_queries, n_neighbors, d_out, true, h->ws, h->qst, s, err,
+                        nullptr);
+  if (rc) return fail(rc, err.msg);
+  return ok();
+}
+
+int fpp_query_dump(fpp_index* h, const float* queries, int n_queries, int n_neighbors, int32_t* out,
+                   float* topk_val, uint32_t* probes, float* probe_val, long long* stats, int32_t* cands,
+                   long long cand_cap) {
+  if (!h) return fail(FPP_ERR_INVALID_ARGUMENT, "query_dump: NULL handle");
+  std::lock_guard<std::mutex> g(h->mu);
+  int rc = check_query_params(h, n_queries, n_neighbors);
+  if (rc) return rc;
+  if (n_queries > 0 && (!queries || !out)) return fail(FPP_ERR_INVALID_ARGUMENT, "query_dump: NULL buffer");
+  if (use_device(h)) return FPP_ERR_CUDA;
+  fpp::QueryDumps dumps;
+  std::vector<long long> cc(n_queries), uc(n_queries);
+  dumps.probes = probes;
+  dumps.probe_v = probe_val;
+  dumps.topk_v = topk_val;
+  dumps.cand_count = cc.data();
+  dumps.unique_count = uc.data();
+  if (cands && cand_cap < 1) return fail(FPP_ERR_INVALID_ARGUMENT, "query_dump: cand_cap must be >= 1");
+  dumps.want_cands = cands != nullptr;
+  fpp::Error err{0, ""};
+  rc = fpp::query_index(h->P, h->di, queries, false, n_queries, n_neighbors, out, false, h->ws, h->qst, h->stream, err,
+                        &dumps);
+  if (rc == FPP_OK && cands) {
+    for (int q = 0; q < n_queries; ++q) {
+      if (uc[q] > cand_cap) return fail(FPP_ERR_INVALID_ARGUMENT, "query_dump: cand_cap smaller than a candidate set");
+      for (long long i = 0; i < cand_cap; ++i)
+        cands[(size_t)q * cand_cap + i] = i < uc[q] ? dumps.cands[(size_t)q * dumps.cand_stride + i] : -1;
+    }
+  }
+  if (rc) return fail(rc, err.msg);
+  if (stats)
+    for (int q = 0; q < n_queries; ++q) {
+      stats[(size_t)q * 4 + 0] = cc[q];
+      stats[(size_t)q * 4 + 1] = uc[q];
+      stats[(size_t)q * 4 + 2] = 0;
+      stats[(size_t)q * 4 + 3] = h->P.qProbes;
+    }
+  return ok();
+}
+
+int fpp_get_info(fpp_index* h, long long* out, int n) {
+  if (!h || !out) return fail(FPP_ERR_INVALID_ARGUMENT, "get_info: NULL argument");
+  std::lock_guard<std::mutex> g(h->mu);
+  const long long v[6] = {h->P.fhtDim,
+                          (long long)h->di.n_ids,
+                          (long long)h->di.max_kept,
+                          (long long)h->P.n_tables * 4LL * h->P.n_proj * h->P.n_proj,
+                          h->built ? 1LL : 0LL,
+                          h->device};
+  for (int i = 0; i < n && i < 6; ++i) out[i] = v[i];
+  return ok();
+}
+
+int fpp_get_stats(fpp_index* h, int kind, double* out, int n) {
+  if (!h || !out) return fail(FPP_ERR_INVALID_ARGUMENT, "get_stats: NULL argument");
+  std::lock_guard<std::mutex> g(h->mu);
+  if (kind == 0) {
+    const fpp::BuildStats& s = h->bst;
+    const double v[8] = {s.ms_center, s.ms_hash, s.ms_sort, s.ms_csr, s.ms_total,
+                         (double)s.n_repaired, (double)s.n_limited, s.points_per_table};
+    for (int i = 0; i < n && i < 8; ++i) out[i] = v[i];
+  } else if (kind == 1) {
+    const fpp::QueryStats& s = h->qst;
+    const double v[6] = {(double)s.total_cand, (double)s.total_unique, (double)s.total_empty,
+                         (double)s.total_probes, (double)s.n_select_ties, (double)s.n_topk_ties};
+    for (int i = 0; i < n && i < 6; ++i) out[i] = v[i];
+  } else {
+    return fail(FPP_ERR_INVALID_ARGUMENT, "get_stats: kind must be 0 or 1");
+  }
+  return ok();
+}
+
+int fpp_dump_bits(fpp_index* h, uint8_t* b1, uint8_t* b2) {
+  if (!h || !b1 || !b2) return fail(FPP_ERR_INVALID_ARGUMENT, "dump_bits: NULL argument");
+  std::lock_guard<std::mutex> g(h->mu);
+  if (!h->built) return fail(FPP_ERR_NOT_BUILT, "dump_bits: the index is not built");
+  memcpy(b1, h->bits.b1.data(), h->bits.b1.size());
+  memcpy(b2, h->bits.b2.data(), h->bits.b2.size());
+  return ok();
+}
+
+int fpp_dump_center(fpp_index* h, float* center) {
+  if (!h || !center) return fail(FPP_ERR_INVALID_ARGUMENT, "dump_center: NULL argument");
+  std::lock_guard<std::mutex> g(h->mu);
+  if (!h->built) return fail(FPP_ERR_NOT_BUILT, "dump_center: the index is not built");
+  cudaSetDevice(h->device);
+  if (cudaMemcpy(center, h->di.center, sizeof(float) * h->P.n_features, cudaMemcpyDeviceToHost) != cudaSuccess)
+    return fail(FPP_ERR_CUDA, "dump_center: copy failed");
+  return ok();
+}
+
+int fpp_dump_tables(fpp_index* h, uint32_t* bucket_start, int32_t* ids) {
+  if (!h || !bucket_start || !ids) return fail(FPP_ERR_INVALID_ARGUMENT, "dump_tables: NULL argument");
+  std::lock_guard<std::mutex> g(h->mu);
+  if (!h->built) return fail(FPP_ERR_NOT_BUILT, "dump_tables: the index is not built");
+  cudaSetDevice(h->device);
+  const size_t nb = (size_t)h->P.n_tables * 4 * h->P.n_proj * h->P.n_proj + 1;
+  if (cudaMemcpy(bucket_start, h->di.bucket_off, sizeof(uint32_t) * nb, cudaMemcpyDeviceToHost) != cudaSuccess ||
+      cudaMemcpy(ids, h->di.ids, sizeof(int32_t) * h->di.n_ids, cudaMemcpyDeviceToHost) != cudaSuccess)
+    return fail(FPP_ERR_CUDA, "dump_tables: copy failed");
+  return ok();
+}
+
+void fpp_print_build_report(fpp_index* h) {
+  if (!h) return;
+  std::lock_guard<std::mutex> g(h->mu);
+  print_build(h);
+}
+
+}  // extern "C"

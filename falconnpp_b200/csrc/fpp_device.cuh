@@ -1,0 +1,238 @@
+// fpp_device.cuh — device building blocks shared by the build and query kernels:
+// group-parallel HD3 rotation (random sign + fast Walsh-Hadamard transform),
+// cross-polytope top-p selection with exact tie handling, block scans and the
+// order-preserving float keys.
+//
+// Arithmetic contract (bit-exact with the reference's FP32 path):
+//  * the sign step multiplies by +1 or -1 (src/FalconnPP.cpp:85-89); it is a
+//    flip of the IEEE sign bit here;
+//  * the FWHT is the unnormalised increasing-stride radix-2 transform
+//    (h = 1, 2, 4, ...; (a, b) -> (a + b, a - b)), which is what the
+//    reference's fht_float computes bit for bit (src/fht.h:11);
+//  * all files are compiled without fast-math and with -fmad=false, so no
+//    add is contracted or reassociated.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "fpp_heap.h"
+
+namespace fpp {
+
+constexpr unsigned kFullMask = 0xffffffffu;
+
+// A vector of FHT floats is held by a group of G lanes, E consecutive
+// elements per lane (lane gl holds elements gl*E .. gl*E+E-1).
+template <int FHT>
+struct Geo {
+  static constexpr int E = FHT < 32 ? FHT : 32;
+  static constexpr int G = FHT / E;
+  static constexpr int WORDS = FHT < 32 ? 1 : FHT / 32;  // sign words per vector
+};
+
+__device__ __forceinline__ uint32_t ord_key(float f) { return ord_key_bits(__float_as_uint(f)); }
+
+// In-place FWHT of the group's vector, stages in increasing stride.
+template <int FHT>
+__device__ __forceinline__ void fwht_group(float (&y)[Geo<FHT>::E], int gl) {
+  constexpr int E = Geo<FHT>::E;
+  constexpr int G = Geo<FHT>::G;
+#pragma unroll
+  for (int h = 1; h < E; h <<= 1) {
+#pragma unroll
+    for (int i = 0; i < E; i += 2 * h) {
+#pragma unroll
+      for (int j = i; j < i + h; ++j) {
+        const float a = y[j];
+        const float b = y[j + h];
+        y[j] = __fadd_rn(a, b);
+        y[j + h] = __fsub_rn(a, b);
+      }
+    }
+  }
+#pragma unroll
+  for (int s = 1; s < G; s <<= 1) {
+    const bool upper = (gl & s) != 0;
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      const float o = __shfl_xor_sync(kFullMask, y[e], s);
+      y[e] = upper ? __fsub_rn(o, y[e]) : __fadd_rn(y[e], o);
+    }
+  }
+}
+
+// Flip the signs selected by the lane's flip word (bit e -> element e).
+template <int FHT>
+__device__ __forceinline__ void flip_signs(float (&y)[Geo<FHT>::E], uint32_t w) {
+#pragma unroll
+  for (int e = 0; e < Geo<FHT>::E; ++e)
+    y[e] = __uint_as_float(__float_as_uint(y[e]) ^ (((w >> e) & 1u) << 31));
+}
+
+// Three rounds of (sign, FWHT) for one layer of one table.  `flips` points at
+// the 3 x WORDS flip words of that (layer, table).
+template <int FHT>
+__device__ __forceinline__ void hd3_rotate(float (&y)[Geo<FHT>::E], const uint32_t* flips, int gl) {
+  constexpr int WORDS = Geo<FHT>::WORDS;
+#pragma unroll
+  for (int r = 0; r < 3; ++r) {
+    const uint32_t w = flips[r * WORDS + (FHT < 32 ? 0 : gl)];
+    flip_signs<FHT>(y, w);
+    fwht_group<FHT>(y, gl);
+  }
+}
+
+// Cross-polytope value of a rotated coordinate: sgn(x)*x with sgn(x) = +1
+// for x >= 0 (src/Utilities.h:26-31), and the bucket code r | neg << log2D.
+__device__ __forceinline__ float cp_value(float x) { return (x >= 0.0f) ? x : -x; }
+__device__ __forceinline__ int cp_code(float x, int r, int log2D) {
+  return (x >= 0.0f) ? r : (r | (1 << log2D));
+}
+
+// Canonical "a before b": larger value first, then smaller position.
+__device__ __forceinline__ bool cp_better(float av, int ar, float bv, int br) {
+  return av > bv || (av == bv && ar < br);
+}
+
+// Top-`cnt` of cp_value over coordinates r < D, in canonical order,
+// computed by the G lanes of the group.  Lane gl == 0 writes out_v[t],
+// out_c[t] (bucket code) for t < found and returns found on every lane.
+template <int FHT>
+__device__ __forceinline__ int group_top_cp(const float (&y)[Geo<FHT>::E], int gl, int D, int log2D,
+                                            int cnt, float* out_v, int* out_c) {
+  constexpr int E = Geo<FHT>::E;
+  constexpr int G = Geo<FHT>::G;
+  uint32_t taken = 0;
+  int found = 0;
+  for (int t = 0; t < cnt; ++t) {
+    float bv = -1.0f;
+    int br = 0x7fffffff;
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      const int r = gl * E + e;
+      const float v = cp_value(y[e]);
+      if (r < D && !((taken >> e) & 1u) && cp_better(v, r, bv, br)) {
+        bv = v;
+        br = r;
+      }
+    }
+#pragma unroll
+    for (int s = 1; s < G; s <<= 1) {
+      const float ov = __shfl_xor_sync(kFullMask, bv, s);
+      const int orr = __shfl_xor_sync(kFullMask, br, s);
+      if (cp_better(ov, orr, bv, br)) {
+        bv = ov;
+        br = orr;
+      }
+    }
+    if (br == 0x7fffffff) break;  // fewer than cnt coordinates
+    int code = 0;
+    if (br / E == gl) {
+      const int e = br - gl * E;
+      taken |= 1u << e;
+      float x = 0.0f;
+#pragma unroll
+      for (int k = 0; k < E; ++k)
+        if (k == e) x = y[k];
+      code = cp_code(x, br, log2D);
+    }
+    // the owner lane publishes the code
+    const int owner = (threadIdx.x & 31 & ~(G - 1)) + br / E;
+    code = __shfl_sync(kFullMask, code, owner);
+    if (gl == 0) {
+      out_v[t] = bv;
+      out_c[t] = code;
+    }
+    ++found;
+  }
+  return found;
+}
+
+// Exact replay of the reference's per-layer top-p scan (FalconnPP.cpp:103-156,
+// :386-452) over the dumped coordinates y[0..D).  Writes vec[0..p) in the
+// reference's order (vec[0] = largest).  hv/hi are scratch of size p.
+__device__ __forceinline__ void replay_layer_topp(const float* y, int D, int log2D, int p, float* hv,
+                                                  int* hi, float* vec_v, int* vec_c) {
+  int n = 0;
+  for (int r = 0; r < D; ++r) {
+    const float x = y[r];
+    topp_offer<int>(hv, hi, n, p, cp_value(x), cp_code(x, r, log2D));
+  }
+  for (int k = p - 1; k >= 0; --k) {
+    vec_v[k] = hv[0];
+    vec_c[k] = hi[0];
+    heap_pop<true, int>(hv, hi, n);
+  }
+}
+
+// Block-wide exclusive scan of one value per thread (blockDim.x <= 1024,
+// multiple of 32).  `tmp` holds 32 ints of shared memory.  Returns the
+// exclusive prefix; *total receives the block sum.
+__device__ __forceinline__ long long block_exclusive_scan(long long v, long long* tmp, long long* total) {
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const int nwarps = blockDim.x >> 5;
+  long long x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const long long y = __shfl_up_sync(kFullMask, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) tmp[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    long long w = lane < nwarps ? tmp[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const long long y = __shfl_up_sync(kFullMask, w, o);
+      if (lane >= o) w += y;
+    }
+    tmp[lane] = w;  // inclusive prefix over warps
+  }
+  __syncthreads();
+  const long long before = (warp > 0 ? tmp[warp - 1] : 0) + x - v;
+  if (total) *total = tmp[nwarps - 1];
+  __syncthreads();
+  return before;
+}
+
+// Ascending bitonic sort (all comparators ascending, length need not be a
+// power of two: positions >= len act as +infinity and never move).
+static __device__ __noinline__ void block_bitonic_sort_u32(uint32_t* key, uint32_t* val, int len) {
+  int N = 1;
+  while (N < len) N <<= 1;
+  for (int k = 2; k <= N; k <<= 1) {
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int t = threadIdx.x; t < N / 2; t += blockDim.x) {
+        int lo, hi;
+        if (j == (k >> 1)) {  // mirror step of the stage
+          const int blk = t / j;
+          const int off = t - blk * j;
+          lo = blk * k + off;
+          hi = blk * k + k - 1 - off;
+        } else {
+          const int blk = t / j;
+          lo = blk * 2 * j + (t - blk * j);
+          hi = lo + j;
+        }
+        if (hi < len) {
+          const uint32_t a = key[lo], b = key[hi];
+          if (a > b) {
+            key[lo] = b;
+            key[hi] = a;
+            const uint32_t va = val[lo];
+            val[lo] = val[hi];
+            val[hi] = va;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+}
+
+__device__ __forceinline__ uint32_t ord_key_inv_dev(uint32_t k) {
+  return (k & 0x80000000u) ? (k ^ 0x80000000u) : ~k;
+}
+
+}  // namespace fpp

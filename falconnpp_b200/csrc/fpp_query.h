@@ -1,0 +1,75 @@
+// fpp_query.h — query pipeline entry point and its reusable device workspace.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <vector>
+
+#include "fpp_index.h"
+
+namespace fpp {
+
+// Device buffers kept between calls so repeated queries do not reallocate.
+struct QueryWorkspace {
+  float* Qd = nullptr;
+  size_t cap_Qd = 0;
+  float* list_v = nullptr;
+  size_t cap_list = 0;
+  uint32_t* list_b = nullptr;
+  size_t cap_list_b = 0;
+  uint32_t* probes = nullptr;
+  size_t cap_probes = 0;
+  float* probe_v = nullptr;
+  size_t cap_probe_v = 0;
+  long long* cand = nullptr;
+  size_t cap_cand = 0;
+  int* empty = nullptr;
+  size_t cap_empty = 0;
+  long long* n_unique = nullptr;
+  size_t cap_nu = 0;
+  float* heap_v = nullptr;
+  size_t cap_heap_v = 0;
+  int* heap_i = nullptr;
+  size_t cap_heap_i = 0;
+  uint32_t* bitset = nullptr;  // per-block dedupe bitsets, all zero between queries
+  int bitset_grid = 0;
+  long long bitset_words = 0;
+  uint32_t* uniq = nullptr;
+  size_t cap_uniq = 0;
+  uint32_t* score = nullptr;
+  size_t cap_score = 0;
+  int32_t* out = nullptr;
+  size_t cap_out = 0;
+  float* out_v = nullptr;
+  size_t cap_out_v = 0;
+  int* counters = nullptr;
+  size_t cap_counters = 0;
+  void release();
+};
+
+struct QueryStats {
+  long long total_cand = 0;    // candidates incl. duplicates
+  long long total_unique = 0;  // unique candidates
+  long long total_empty = 0;   // probed empty buckets
+  long long total_probes = 0;
+  int n_select_ties = 0;       // queries whose probe cut needed the exact replay
+  int n_topk_ties = 0;         // queries whose top-k needed the exact replay
+};
+
+// Optional host-side dumps for parity checks (any pointer may be null).
+struct QueryDumps {
+  uint32_t* probes = nullptr;      // [nq][qProbes]
+  float* probe_v = nullptr;        // [nq][qProbes]
+  float* topk_v = nullptr;         // [nq][k]
+  long long* cand_count = nullptr; // [nq]
+  long long* unique_count = nullptr;
+  bool want_cands = false;         // unique candidate ids per query (unordered)
+  std::vector<int32_t> cands;      // out: [nq][cand_stride], valid up to unique_count
+  long long cand_stride = 0;
+};
+
+int query_index(const Params& P, const DeviceIndex& di, const float* Q, bool q_on_device, int nq, int k,
+                int32_t* out, bool out_on_device, QueryWorkspace& ws, QueryStats& st, cudaStream_t s,
+                Error& err, QueryDumps* dumps);
+
+}  // namespace fpp

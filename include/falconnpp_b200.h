@@ -1,0 +1,135 @@
+/* falconnpp_b200.h — C ABI of the B200 Falconn++ index (one GPU).
+ *
+ * Every entry point is plain C: opaque handle, plain pointers and sizes, and
+ * an int status (0 = success, negative = error; fpp_last_error() then returns
+ * a message for the calling thread).  Matrices use the reference's layout:
+ * a d x n column-major float32 matrix, i.e. n points of d contiguous floats.
+ *
+ * Each function names the reference interface it replaces (paths relative to
+ * the reference project root).  Calls on one handle are serialised.
+ */
+#ifndef FALCONNPP_B200_H
+#define FALCONNPP_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct fpp_index fpp_index;
+
+enum {
+  FPP_OK = 0,
+  FPP_ERR_INVALID_ARGUMENT = -1,
+  FPP_ERR_NOT_BUILT = -2,
+  FPP_ERR_CUDA = -3,
+  FPP_ERR_OUT_OF_MEMORY = -4,
+  FPP_ERR_UNSUPPORTED = -5,
+  FPP_ERR_NON_FINITE = -6,
+  FPP_ERR_DEVICE = -7
+};
+
+/* Replaces FalconnPP::FalconnPP(int n, int d), src/FalconnPP.h:80-83
+ * (python: FalconnPP(n_points, n_features), python/python_wrapper.cpp:16).
+ * Binds the handle to the current CUDA device. */
+int fpp_create(int n_points, int n_features, fpp_index** out);
+
+/* Replaces FalconnPP::~FalconnPP, src/FalconnPP.h:131.  Frees all device memory. */
+void fpp_destroy(fpp_index* h);
+
+/* Replaces FalconnPP::Index2Layers, src/FalconnPP.h:85-100
+ * (python: setIndexParam(n_tables, n_proj, bucket_minSize, bucket_scale, iProbes,
+ * n_threads=8, random_seed=-1), python/python_wrapper.cpp:19-22).
+ * random_seed = -1 seeds from the wall clock exactly like the reference.
+ * Rejects what the reference leaves undefined: n_proj not a power of two,
+ * fhtDim > 1024, iProbes outside [1, min(32, n_proj)]. */
+int fpp_set_index_param(fpp_index* h, int n_tables, int n_proj, int bucket_minSize, float bucket_scale,
+                        int iProbes, int n_threads, int random_seed);
+
+/* Replaces FalconnPP::set_qProbes, src/FalconnPP.h:113-115. */
+int fpp_set_qprobes(fpp_index* h, int qProbes);
+
+/* Replaces FalconnPP::set_threads, src/FalconnPP.h:117-123.  Stored and
+ * reported; the GPU path does not use host threads. */
+int fpp_set_threads(fpp_index* h, int n_threads);
+
+/* Replaces FalconnPP::clear, src/FalconnPP.h:102-111. */
+int fpp_clear(fpp_index* h);
+
+/* Replaces FalconnPP::build2Layers_1D, src/FalconnPP.cpp:21-303
+ * (python: build(dataset), python/python_wrapper.cpp:28).
+ * dataset: host memory, d x n column-major float32 (n points of d floats). */
+int fpp_build(fpp_index* h, const float* dataset);
+
+/* Same as fpp_build with the dataset already in device memory; stream may be
+ * NULL (the handle's own stream).  Returns after the index is complete. */
+int fpp_build_device(fpp_index* h, const float* d_dataset, void* stream);
+
+/* Replaces FalconnPP::query2Layers_1D, src/FalconnPP.cpp:310-707
+ * (python: query(queries, n_neighbors, verbose=False), python/python_wrapper.cpp:29-30).
+ * queries: host, d x n_queries column-major; out: host, n_queries x n_neighbors
+ * int32 row-major, each row in descending inner product, 0-padded.
+ * verbose = 1 prints the reference's statistics and writes its
+ * 1D_Top_<k>_D_..._qProbe_<q>.txt file to the working directory
+ * (FalconnPP.cpp:682-703). */
+int fpp_query(fpp_index* h, const float* queries, int n_queries, int n_neighbors, int verbose, int32_t* out);
+
+/* Same as fpp_query with queries and out in device memory; asynchronous with
+ * respect to the host only as far as the kernels allow (the call returns once
+ * the results are written).  stream may be NULL. */
+int fpp_query_device(fpp_index* h, const float* d_queries, int n_queries, int n_neighbors, int32_t* d_out,
+                     void* stream);
+
+/* Message of the last failing call on this thread ("" if none). */
+const char* fpp_last_error(void);
+
+/* Index facts: out[0] fhtDim, out[1] stored ids, out[2] largest stored bucket,
+ * out[3] buckets (n_tables * 4 * n_proj^2), out[4] built (0/1), out[5] device. */
+int fpp_get_info(fpp_index* h, long long* out, int n);
+
+/* Statistics of the last build (kind 0) or query (kind 1) as doubles.
+ * build: ms_center, ms_hash, ms_sort, ms_csr, ms_total, repaired buckets,
+ *        limited buckets (FalconnPP.cpp:241), points per table / n (:296);
+ * query: candidates, unique candidates, empty probed buckets, probes,
+ *        probe-cut replays, top-k replays (all summed over the queries). */
+int fpp_get_stats(fpp_index* h, int kind, double* out, int n);
+
+/* Tuning and test switches: "exact_bucket_order" (default 1: bucket contents
+ * in the reference's heap order even among equal scores; 0: ascending id among
+ * equal scores, the kept set is identical either way), "tables_per_chunk". */
+int fpp_set_option(fpp_index* h, const char* key, long long value);
+
+/* Prints the build report the reference writes to stdout after
+ * build2Layers_1D (src/FalconnPP.cpp:23-30, :275-301) for the last build. */
+void fpp_print_build_report(fpp_index* h);
+
+/* Parity dumps (host buffers).
+ * fpp_dump_bits: bitHD1/bitHD2 (src/FalconnPP.h:61-68), n_tables*3*fhtDim bytes each.
+ * fpp_dump_center: the d floats subtracted from the data (FalconnPP.cpp:33).
+ * fpp_dump_tables: bucket_start[n_buckets+1] (CSR offsets, bucket size =
+ *   difference, equal to the reference's uint16 bucket size) and ids[stored ids]. */
+int fpp_dump_bits(fpp_index* h, uint8_t* bitHD1, uint8_t* bitHD2);
+int fpp_dump_center(fpp_index* h, float* center);
+int fpp_dump_tables(fpp_index* h, uint32_t* bucket_start, int32_t* ids);
+
+/* fpp_build with the per-(table, point) hash codes captured: codes/scores are
+ * [n_tables][n_points][iProbes] in the drain order of the reference's minQue
+ * (FalconnPP.cpp:196-201). */
+int fpp_build_dump_hash(fpp_index* h, const float* dataset, int32_t* codes, float* scores);
+
+/* fpp_query with intermediate results captured (any pointer may be NULL):
+ * topk_val [nq][k] scores; probes / probe_val [nq][qProbes] probed global
+ * bucket ids (the probed set; its order is the pop order only where scores
+ * differ); stats [nq][4] = candidates, unique candidates, empty buckets,
+ * probes; cands [nq][cand_cap] the unique candidate ids (unordered, -1 padded).
+ * cand_cap must be at least the largest unique-candidate count of the batch. */
+int fpp_query_dump(fpp_index* h, const float* queries, int n_queries, int n_neighbors, int32_t* out,
+                   float* topk_val, uint32_t* probes, float* probe_val, long long* stats, int32_t* cands,
+                   long long cand_cap);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FALCONNPP_B200_H */
