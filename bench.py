@@ -1,0 +1,399 @@
+#!/usr/bin/env python
+"""Query throughput of the B200 Falconn++ index (QPS at recall@20 >= 0.9).
+
+Workload (one step = one pass of the query path over one batch): the 1M x 200
+synthetic MIPS index (Gaussian mixture, 256 centres, sigma 0.3, log-normal(0,
+0.4) norms; L=100 tables, n_proj=256, bucket_minSize=1000, alpha=0.01,
+iProbes=3) queried with a batch of 10,000 held-out queries, k=20.  qProbes is
+the smallest of {10, 20, 40, 80} whose recall@20 against the FP64 exact top-20
+(on a 500-query sample) is >= 0.90.
+
+* ``value``: queries/s over all ranks with queries and index resident in HBM
+  (device pointers through fpp_query_device), CUDA events around K steps;
+* ``e2e``: the same through fpp_query with pinned host buffers, the query
+  upload and the result download inside the timed region;
+* ``roofline``: the gather/rerank kernel's algorithmic bytes per launch over its
+  CUDA-event duration, against the measured HBM copy bandwidth;
+* ``cpu_baseline``: the CPU restatement (oracle) of the reference's query
+  path on the same index, all host threads.
+
+``--impl reference`` times the reference's CPU path (the oracle port, which
+builds its own index on the host cores) on the same workload.  Multi-GPU runs
+(torchrun) are replicas: every rank holds the full index and answers its own
+batch of queries (weak scaling); no collective touches the data path.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    "mips-1Mx200-L100": dict(n=1_000_000, d=200, n_centres=256, norm_sigma=0.4, L=100, D=256, minSize=1000,
+                             alpha=0.01, iProbes=3, nq=10_000, k=20, sweep=(10, 20, 40, 80)),
+    # small case of the same kernels for profiler captures (index > L2, ~1 GB on the device)
+    "mips-300Kx200-L100-small": dict(n=300_000, d=200, n_centres=256, norm_sigma=0.4, L=100, D=256, minSize=1000,
+                                     alpha=0.01, iProbes=3, nq=2_000, k=20, sweep=(10,)),
+}
+INDEX_SEED = 42
+RECALL_SAMPLE = 500
+RECALL_TARGET = 0.90
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            j = json.load(f)
+        return float(j["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            time.sleep(0.3)
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in getattr(self, "lines", []):
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": mx, "reasons": ["unavailable"], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def make_data(w, rank):
+    from falconnpp_b200 import synth
+    X = synth.mixture(w["n"], w["d"], n_centres=w["n_centres"], norm_sigma=w["norm_sigma"], seed=0)
+    Q = synth.mixture(w["nq"], w["d"], n_centres=w["n_centres"], norm_sigma=w["norm_sigma"], seed=1 + 1000 * rank)
+    return X, Q
+
+
+def exact_topk_fp64(X_dev, Q_np, k):
+    """FP64 exact MIPS top-k of a query sample (measurement only)."""
+    import torch
+    out = []
+    Xd = X_dev.double()
+    for s in range(0, Q_np.shape[0], 100):
+        q = torch.from_numpy(Q_np[s:s + 100]).cuda().double()
+        sc = q @ Xd.T
+        out.append(torch.topk(sc, k, dim=1).indices.int().cpu().numpy())
+    del Xd
+    return np.concatenate(out)
+
+
+def recall(truth, ans, k):
+    from falconnpp_b200 import synth
+    return synth.recall_at_k(truth, ans, k)
+
+
+def run_ours(args, w, rank, world, local_rank):
+    import torch
+    from falconnpp_b200 import capi
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist  # noqa: F811
+    X, Q = make_data(w, rank)
+    n, d, nq, k = w["n"], w["d"], w["nq"], w["k"]
+    idx = capi.Index(n, d)
+    idx.set_index_param(w["L"], w["D"], w["minSize"], w["alpha"], w["iProbes"], 8, INDEX_SEED)
+    Xd = torch.from_numpy(X).cuda()
+    t0 = time.perf_counter()
+    idx.build_device(Xd.data_ptr(), torch.cuda.current_stream().cuda_stream)
+    build_s = time.perf_counter() - t0
+    bstats = idx.stats(0)
+    Qd = torch.from_numpy(Q).cuda()
+    outd = torch.empty((nq, k), dtype=torch.int32, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+
+    # qProbes: smallest of the sweep reaching the recall target on the sample
+    ns = min(RECALL_SAMPLE, nq)
+    truth = exact_topk_fp64(Xd, Q[:ns], k)
+    chosen, rec = None, None
+    sweep_log = {}
+    for qp in w["sweep"]:
+        idx.set_qprobes(qp)
+        idx.query_device(Qd.data_ptr(), nq, k, outd.data_ptr(), stream)
+        r = recall(truth, outd[:ns].cpu().numpy(), k)
+        sweep_log[qp] = round(r, 4)
+        if chosen is None and r >= RECALL_TARGET:
+            chosen, rec = qp, r
+    if chosen is None:
+        chosen, rec = w["sweep"][-1], sweep_log[w["sweep"][-1]]
+    idx.set_qprobes(chosen)
+    del Xd
+    torch.cuda.empty_cache()
+
+    # device-resident timing
+    for _ in range(args.warmup):
+        idx.query_device(Qd.data_ptr(), nq, k, outd.data_ptr(), stream)
+    torch.cuda.synchronize()
+    idx.set_option("stage_timing", 1)
+    step_ms, rerank_ms, launches, uniq, cand = [], [], 0, 0.0, 0.0
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local_rank) as clk:
+        ev0.record()
+        for _ in range(args.steps):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            idx.query_device(Qd.data_ptr(), nq, k, outd.data_ptr(), stream)
+            e1.record()
+            st = idx.stats(1)
+            launches += int(st[6])
+            rerank_ms.append(st[9])
+            uniq += st[1]
+            cand += st[0]
+            e1.synchronize()
+            step_ms.append(e0.elapsed_time(e1))
+        ev1.record()
+        torch.cuda.synchronize()
+    total_ms = ev0.elapsed_time(ev1)
+    if dist:
+        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    idx.set_option("stage_timing", 0)
+    value = world * nq * args.steps / (total_ms / 1000.0)
+
+    # end to end through the C ABI with pinned host buffers
+    Qh = torch.from_numpy(Q).pin_memory()
+    outh = torch.empty((nq, k), dtype=torch.int32).pin_memory()
+    for _ in range(max(1, args.warmup // 2)):
+        capi.lib().fpp_query(idx.h, Qh.data_ptr(), nq, k, 0, outh.data_ptr())
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        rc = capi.lib().fpp_query(idx.h, Qh.data_ptr(), nq, k, 0, outh.data_ptr())
+        if rc != 0:
+            raise RuntimeError(capi.lib().fpp_last_error().decode())
+    e2e_s = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = world * nq * args.steps / e2e_s
+    assert np.array_equal(outh.numpy(), outd.cpu().numpy()), "host and device query paths disagree"
+
+    # roofline of the gather/rerank kernel (one launch per step)
+    steps = args.steps
+    avg_rerank_s = statistics.mean(rerank_ms) / 1000.0
+    bytes_per_launch = (uniq / steps) * d * 4 + (cand / steps) * 4 + nq * chosen * 8 + nq * (4 * d + 4 * k)
+    peak, peak_kind = measured_peaks()
+    achieved = bytes_per_launch / avg_rerank_s / 1e9
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "k_gather_rerank.traffic.json")
+    if os.path.exists(prof):
+        with open(prof) as f:
+            pj = json.load(f)
+        traffic = pj["dram_bytes_per_unique_row"] * (uniq / steps)
+
+    result = {
+        "metric": "QPS @ recall@20>=0.9 (1M x 200 MIPS, plain FP32 form); p99 ms per 10k-query batch",
+        "value": round(value, 1),
+        "unit": "queries/s",
+        "n_gpus": world,
+        "steps": steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(total_ms / steps, 4),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": args.workload, "n_points": n, "d": d, "n_tables": w["L"], "n_proj": w["D"],
+                   "iProbes": w["iProbes"], "bucket_minSize": w["minSize"], "bucket_scale": w["alpha"],
+                   "queries_per_step": nq, "k": k, "qProbes": chosen, "form": "plain-fp32",
+                   "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (index 1.9 GB)"},
+        "recall_at_k": round(rec, 4),
+        "recall_sweep": sweep_log,
+        "latency_ms": {"p50": round(float(np.percentile(step_ms, 50)), 4),
+                       "p99": round(float(np.percentile(step_ms, 99)), 4),
+                       "unit": "per 10k-query batch"},
+        "build_s": round(build_s, 3),
+        "build_breakdown_ms": {"center": round(bstats[0], 1), "hash": round(bstats[1], 1),
+                               "sort": round(bstats[2], 1), "csr": round(bstats[3], 1)},
+        "e2e": {"value": round(e2e, 1), "unit": "queries/s", "h2d_bytes_per_step": nq * d * 4,
+                "d2h_bytes_per_step": nq * k * 4},
+        "gpu_launches": launches,
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "traffic": traffic, "peak_kind": peak_kind,
+                     "kernel": "k_gather_rerank",
+                     "bytes_per_launch": int(bytes_per_launch), "avg_launch_ms": round(avg_rerank_s * 1e3, 4)},
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        result["cpu_baseline"] = cpu_baseline_from_index(idx, X, Q, w, chosen)
+    return result
+
+
+def cpu_baseline_from_index(idx, X, Q, w, qprobes):
+    """The oracle's query path (the reference's algorithm on the host cores)
+    on the same index, over the same batch of queries."""
+    from oracle import oracle
+    o = oracle.Index(w["n"], w["d"])
+    threads = os.cpu_count() or 1
+    o.set_index_param(w["L"], w["D"], w["minSize"], w["alpha"], w["iProbes"], threads, INDEX_SEED)
+    center = idx.dump_center()
+    b1, b2 = idx.dump_bits()
+    start, ids = idx.dump_tables()
+    Xc = X - center[None, :]
+    o.import_index(Xc, center, b1, b2, start, ids)
+    o.set_qprobes(qprobes)
+    nsamp = min(Q.shape[0], 4000)
+    t0 = time.perf_counter()
+    o.query(Q[:nsamp], w["k"])
+    dt = time.perf_counter() - t0
+    return {"value": round(nsamp / dt, 1), "unit": "queries/s", "cores": threads, "kind": "port",
+            "sample": f"{nsamp} of the step's {Q.shape[0]} queries on the same index, qProbes={qprobes}"}
+
+
+def run_reference(args, w):
+    """The reference's CPU path: the oracle port builds its own index on the
+    host cores and answers a bounded sample of the batch per step."""
+    from oracle import oracle
+    X, Q = make_data(w, 0)
+    threads = os.cpu_count() or 1
+    o = oracle.Index(w["n"], w["d"])
+    o.set_index_param(w["L"], w["D"], w["minSize"], w["alpha"], w["iProbes"], threads, INDEX_SEED)
+    t0 = time.perf_counter()
+    o.build(X)
+    build_s = time.perf_counter() - t0
+    qp = args.qprobes or w["sweep"][0]
+    o.set_qprobes(qp)
+    nsamp = min(Q.shape[0], 2000)
+    for _ in range(args.warmup):
+        o.query(Q[:200], w["k"])
+    ts = []
+    for s in range(args.steps):
+        sl = Q[(s * nsamp) % Q.shape[0]:][:nsamp]
+        t0 = time.perf_counter()
+        o.query(sl, w["k"])
+        ts.append(time.perf_counter() - t0)
+    total = sum(ts)
+    value = nsamp * args.steps / total
+    return {
+        "metric": "QPS @ recall@20>=0.9 (1M x 200 MIPS, plain FP32 form); p99 ms per 10k-query batch",
+        "impl": "reference",
+        "value": round(value, 1),
+        "unit": "queries/s",
+        "n_gpus": 0,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(1000 * total / args.steps, 3),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": args.workload, "n_points": w["n"], "d": w["d"], "n_tables": w["L"],
+                   "n_proj": w["D"], "iProbes": w["iProbes"], "qProbes": qp, "k": w["k"],
+                   "queries_per_step": nsamp, "form": "reference CPU path (oracle port, OpenMP)"},
+        "build_s": round(build_s, 2),
+        "cpu_baseline": {"value": round(value, 1), "unit": "queries/s", "cores": threads, "kind": "port",
+                         "sample": f"{nsamp} queries per step of the 10k-query batch"},
+        "e2e": {"value": round(value, 1), "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", default="mips-1Mx200-L100", choices=sorted(WORKLOADS))
+    ap.add_argument("--qprobes", type=int, default=0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    w = WORKLOADS[args.workload]
+    if args.qprobes:
+        w = dict(w, sweep=(args.qprobes,))
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        print(json.dumps(run_reference(args, w)), flush=True)
+        return 0
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    res = run_ours(args, w, rank, world, local_rank)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(res), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -152,8 +152,8 @@ class Index:
                     device=int(v[5]))
 
     def stats(self, kind: int) -> np.ndarray:
-        v = np.zeros(8, np.float64)
-        _check(lib().fpp_get_stats(self.h, kind, _ptr(v), 8))
+        v = np.zeros(10, np.float64)
+        _check(lib().fpp_get_stats(self.h, kind, _ptr(v), 10))
         return v
 
     def dump_bits(self):

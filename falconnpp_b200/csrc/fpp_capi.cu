@@ -252,6 +252,8 @@ int fpp_set_option(fpp_index* h, const char* key, long long value) {
   std::lock_guard<std::mutex> g(h->mu);
   if (!strcmp(key, "exact_bucket_order")) {
     h->opt.exact_bucket_order = value != 0;
+  } else if (!strcmp(key, "stage_timing")) {
+    h->ws.stage_timing = value != 0;
   } else if (!strcmp(key, "tables_per_chunk")) {
     if (value < 0) return fail(FPP_ERR_INVALID_ARGUMENT, "set_option: tables_per_chunk must be >= 0");
     h->opt.tables_per_chunk = (int)value;
@@ -398,9 +400,10 @@ int fpp_get_stats(fpp_index* h, int kind, double* out, int n) {
     for (int i = 0; i < n && i < 8; ++i) out[i] = v[i];
   } else if (kind == 1) {
     const fpp::QueryStats& s = h->qst;
-    const double v[6] = {(double)s.total_cand, (double)s.total_unique, (double)s.total_empty,
-                         (double)s.total_probes, (double)s.n_select_ties, (double)s.n_topk_ties};
-    for (int i = 0; i < n && i < 6; ++i) out[i] = v[i];
+    const double v[10] = {(double)s.total_cand, (double)s.total_unique, (double)s.total_empty,
+                          (double)s.total_probes, (double)s.n_select_ties, (double)s.n_topk_ties,
+                          (double)s.launches, s.ms_hash, s.ms_select, s.ms_rerank};
+    for (int i = 0; i < n && i < 10; ++i) out[i] = v[i];
   } else {
     return fail(FPP_ERR_INVALID_ARGUMENT, "get_stats: kind must be 0 or 1");
   }

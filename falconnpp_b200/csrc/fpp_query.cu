@@ -606,7 +606,11 @@ void QueryWorkspace::release() {
   cudaFree(out);
   cudaFree(out_v);
   cudaFree(counters);
+  for (auto& e : ev)
+    if (e) cudaEventDestroy(e);
+  const bool timing = stage_timing;
   *this = QueryWorkspace();
+  stage_timing = timing;
 }
 
 int query_index(const Params& P, const DeviceIndex& di, const float* Q, bool q_on_device, int nq, int k,
@@ -659,6 +663,10 @@ int query_index(const Params& P, const DeviceIndex& di, const float* Q, bool q_o
     if ((e = ensure(ws.out_v, ws.cap_out_v, (size_t)nq * k)) != cudaSuccess) return fail(e, "alloc");
   if ((e = cudaMemsetAsync(ws.counters, 0, sizeof(int) * 4, s)) != cudaSuccess) return fail(e, "memset");
 
+  if (ws.stage_timing && !ws.ev[0])
+    for (auto& ev : ws.ev)
+      if ((e = cudaEventCreate(&ev)) != cudaSuccess) return fail(e, "event create");
+  if (ws.stage_timing) cudaEventRecord(ws.ev[0], s);
   // 1. rotate + hash every (query, table)
   {
     // heap scratch: pair heaps of k_query_hash (one per concurrent group) and
@@ -704,8 +712,10 @@ int query_index(const Params& P, const DeviceIndex& di, const float* Q, bool q_o
     sa.cand = ws.cand;
     sa.empty = ws.empty;
     sa.n_tie = ws.counters + 0;
+    if (ws.stage_timing) cudaEventRecord(ws.ev[1], s);
     k_probe_select<<<grid, 256, 0, s>>>(sa, ws.heap_v, ws.heap_i);
     if ((e = cudaGetLastError()) != cudaSuccess) return fail(e, "k_probe_select");
+    if (ws.stage_timing) cudaEventRecord(ws.ev[2], s);
   }
   // 3. scratch sizing: the largest candidate count of the batch
   std::vector<long long> hcand(nq);
@@ -764,8 +774,11 @@ int query_index(const Params& P, const DeviceIndex& di, const float* Q, bool q_o
   }
   ra.cand_dump = cand_dev;
   ra.n_tie = ws.counters + 1;
+  if (ws.stage_timing) cudaEventRecord(ws.ev[3], s);
   k_gather_rerank<<<grid, kRrThreads, 0, s>>>(ra);
   if ((e = cudaGetLastError()) != cudaSuccess) return fail(e, "k_gather_rerank");
+  if (ws.stage_timing) cudaEventRecord(ws.ev[4], s);
+  st.launches = 3;
   if (!out_on_device) {
     if ((e = cudaMemcpyAsync(out, ws.out, sizeof(int32_t) * nq * k, cudaMemcpyDeviceToHost, s)) != cudaSuccess)
       return fail(e, "copy out");
@@ -797,6 +810,15 @@ int query_index(const Params& P, const DeviceIndex& di, const float* Q, bool q_o
     st.total_empty += hempty[i];
   }
   st.total_probes = (long long)nq * Qp;
+  if (ws.stage_timing) {
+    float a = 0, b = 0, c = 0;
+    cudaEventElapsedTime(&a, ws.ev[0], ws.ev[1]);
+    cudaEventElapsedTime(&b, ws.ev[1], ws.ev[2]);
+    cudaEventElapsedTime(&c, ws.ev[3], ws.ev[4]);
+    st.ms_hash = a;
+    st.ms_select = b;
+    st.ms_rerank = c;
+  }
   st.n_select_ties = hc[0];
   st.n_topk_ties = hc[1];
   if (dumps && dumps->unique_count) memcpy(dumps->unique_count, hu.data(), sizeof(long long) * nq);

@@ -44,6 +44,8 @@ struct QueryWorkspace {
   size_t cap_out_v = 0;
   int* counters = nullptr;
   size_t cap_counters = 0;
+  bool stage_timing = false;
+  cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
   void release();
 };
 
@@ -54,6 +56,9 @@ struct QueryStats {
   long long total_probes = 0;
   int n_select_ties = 0;       // queries whose probe cut needed the exact replay
   int n_topk_ties = 0;         // queries whose top-k needed the exact replay
+  long long launches = 0;      // kernels launched by the call
+  // CUDA-event durations on the launching stream (only with stage timing on)
+  double ms_hash = 0, ms_select = 0, ms_rerank = 0;
 };
 
 // Optional host-side dumps for parity checks (any pointer may be null).

@@ -92,12 +92,15 @@ int fpp_get_info(fpp_index* h, long long* out, int n);
  * build: ms_center, ms_hash, ms_sort, ms_csr, ms_total, repaired buckets,
  *        limited buckets (FalconnPP.cpp:241), points per table / n (:296);
  * query: candidates, unique candidates, empty probed buckets, probes,
- *        probe-cut replays, top-k replays (all summed over the queries). */
+ *        probe-cut replays, top-k replays (all summed over the queries),
+ *        kernels launched, then (with the "stage_timing" option) the CUDA-event
+ *        milliseconds of the hashing, probe-selection and gather/rerank kernels. */
 int fpp_get_stats(fpp_index* h, int kind, double* out, int n);
 
 /* Tuning and test switches: "exact_bucket_order" (default 1: bucket contents
  * in the reference's heap order even among equal scores; 0: ascending id among
- * equal scores, the kept set is identical either way), "tables_per_chunk". */
+ * equal scores, the kept set is identical either way), "tables_per_chunk",
+ * "stage_timing" (0/1: CUDA events around each query kernel). */
 int fpp_set_option(fpp_index* h, const char* key, long long value);
 
 /* Prints the build report the reference writes to stdout after

@@ -331,6 +331,25 @@ long long orc_build(void* h, const float* X) {
   return (long long)pos;
 }
 
+// Load an index built elsewhere (centred data, centre, signs, CSR tables) so
+// the oracle's query path can be timed or checked without rebuilding.
+void orc_import(void* h, const float* Xc, const float* center, const uint8_t* b1, const uint8_t* b2,
+                const uint32_t* start, const int* ids, long long n_ids) {
+  Index& I = *static_cast<Index*>(h);
+  const size_t n = I.n_points, d = I.n_features;
+  const size_t nb = (size_t)I.n_tables * 4 * I.n_proj * I.n_proj;
+  const size_t nbits = (size_t)I.fhtDim * I.n_tables * I.n_rotate;
+  I.X.assign(Xc, Xc + n * d);
+  I.center.assign(center, center + d);
+  I.bitHD1.assign(b1, b1 + nbits);
+  I.bitHD2.assign(b2, b2 + nbits);
+  I.bucketStart.resize(nb + 1);
+  I.bucketSize.resize(nb);
+  for (size_t g = 0; g <= nb; ++g) I.bucketStart[g] = start[g];
+  for (size_t g = 0; g < nb; ++g) I.bucketSize[g] = (uint16_t)(start[g + 1] - start[g]);
+  I.tables.assign(ids, ids + n_ids);
+}
+
 // Accessors for the built index (sizes are known to the caller).
 void orc_get_center(void* h, float* out) {
   Index& I = *static_cast<Index*>(h);

@@ -53,6 +53,7 @@ def lib() -> ctypes.CDLL:
             "orc_query": (i32, [vp, vp, i32, i32, vp, vp, vp, vp, vp]),
             "orc_query_candidates": (i64, [vp, vp, vp, i64]),
             "orc_bf_topk_f64": (None, [vp, i64, i32, vp, i32, i32, i32, vp]),
+            "orc_import": (None, [vp, vp, vp, vp, vp, vp, vp, i64]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -140,6 +141,15 @@ class Index:
         X = np.ascontiguousarray(X, np.float32)
         self.n_ids = int(lib().orc_build(self.h, _p(X)))
         return self.n_ids
+
+    def import_index(self, Xc, center, b1, b2, start, ids):
+        """Adopt an index built elsewhere (e.g. dumped from the GPU)."""
+        self._keep = [np.ascontiguousarray(a) for a in (Xc, center, b1, b2)]
+        start = np.ascontiguousarray(start, np.uint32)
+        ids = np.ascontiguousarray(ids, np.int32)
+        lib().orc_import(self.h, _p(self._keep[0]), _p(self._keep[1]), _p(self._keep[2]), _p(self._keep[3]),
+                         _p(start), _p(ids), len(ids))
+        self.n_ids = len(ids)
 
     def center(self):
         c = np.zeros(self.d, np.float32)
