@@ -18,10 +18,11 @@ EXPORTED = [
     "fpp_create", "fpp_destroy", "fpp_set_index_param", "fpp_set_qprobes", "fpp_set_threads", "fpp_clear",
     "fpp_build", "fpp_build_device", "fpp_query", "fpp_query_device", "fpp_last_error", "fpp_get_info",
     "fpp_get_stats", "fpp_set_option", "fpp_print_build_report", "fpp_dump_bits", "fpp_dump_center",
-    "fpp_dump_tables", "fpp_build_dump_hash", "fpp_query_dump",
+    "fpp_dump_tables", "fpp_build_dump_hash", "fpp_query_dump", "fpp_rerank_probes_noalloc",
 ]
 
 _lib = None
+FPP_ERR_INVALID_ARGUMENT = -1
 
 
 class FppError(RuntimeError):
@@ -57,6 +58,7 @@ def lib() -> ctypes.CDLL:
             "fpp_dump_tables": (i32, [vp, vp, vp]),
             "fpp_build_dump_hash": (i32, [vp, vp, vp, vp]),
             "fpp_query_dump": (i32, [vp, vp, i32, i32, vp, vp, vp, vp, vp, vp, i64]),
+            "fpp_rerank_probes_noalloc": (i32, [vp, vp, i32, vp, i32, i32, vp, vp]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)

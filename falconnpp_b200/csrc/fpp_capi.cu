@@ -23,20 +23,7 @@
 #include "fpp_index.h"
 #include "fpp_query.h"
 
-struct fpp_index {
-  fpp::Params P;
-  fpp::DeviceIndex di;
-  fpp::QueryWorkspace ws;
-  fpp::HostBits bits;
-  fpp::BuildOptions opt;
-  fpp::BuildStats bst;
-  fpp::QueryStats qst;
-  bool params_set = false;
-  bool built = false;
-  int device = 0;
-  cudaStream_t stream = nullptr;
-  std::mutex mu;
-};
+#include "fpp_handle.h"
 
 namespace {
 
@@ -154,6 +141,13 @@ void print_build(const fpp_index* h) {
 }
 
 }  // namespace
+
+namespace fpp {
+// Lets the other translation units of the library report an error through
+// fpp_last_error().
+int set_last_error(int code, const std::string& msg) { return fail(code, msg); }
+int clear_last_error() { return ok(); }
+}  // namespace fpp
 
 extern "C" {
 

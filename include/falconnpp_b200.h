@@ -131,6 +131,25 @@ int fpp_query_dump(fpp_index* h, const float* queries, int n_queries, int n_neig
                    float* topk_val, uint32_t* probes, float* probe_val, long long* stats, int32_t* cands,
                    long long cand_cap);
 
+/* No counterpart in the reference.  The gather, deduplicate, rerank and top-k
+ * stage of fpp_query for callers that cannot allocate device memory: code
+ * recording a CUDA graph, a serving thread that must not stall on cudaMalloc /
+ * cudaFree (they synchronise the device), or a host process whose device
+ * memory belongs to another allocator.  It allocates nothing: its scratch is
+ * a 64 MiB __device__ array that every GPU loading the library holds until
+ * exit.  d_queries: n_queries x n_features floats; d_probes: n_queries x
+ * n_probes global bucket ids (the probes fpp_query_dump reports); d_out:
+ * n_queries x n_neighbors int32, the same top-k fpp_query gives for those
+ * probes.  All three in device memory.  The first call on a device looks up
+ * the scratch address; make it before any stream capture.  Calls whose
+ * kernels overlap on one GPU race on the shared scratch.  Rejects
+ * n_neighbors > 1024, n_features > 1024, n_points beyond the scratch (about
+ * 500M), and queries with more unique candidates than a block's share
+ * (65536 when n_points allows; the row is zeroed and an error returned).
+ * Returns after the results are written. */
+int fpp_rerank_probes_noalloc(fpp_index* h, const float* d_queries, int n_queries, const uint32_t* d_probes,
+                              int n_probes, int n_neighbors, int32_t* d_out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
