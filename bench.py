@@ -115,10 +115,26 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def query_seed(rank: int) -> int:
+    """Each replica answers its own batch: rank r draws its queries with seed 1 + 1000 r."""
+    return 1 + 1000 * rank
+
+
+def reduce_max(x: float, device: str = "cuda") -> float:
+    """Max over ranks (every rank calls it the same number of times)."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return x
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def make_data(w, rank):
     from falconnpp_b200 import synth
     X = synth.mixture(w["n"], w["d"], n_centres=w["n_centres"], norm_sigma=w["norm_sigma"], seed=0)
-    Q = synth.mixture(w["nq"], w["d"], n_centres=w["n_centres"], norm_sigma=w["norm_sigma"], seed=1 + 1000 * rank)
+    Q = synth.mixture(w["nq"], w["d"], n_centres=w["n_centres"], norm_sigma=w["norm_sigma"], seed=query_seed(rank))
     return X, Q
 
 
@@ -207,11 +223,7 @@ def run_ours(args, w, rank, world, local_rank):
             step_ms.append(e0.elapsed_time(e1))
         ev1.record()
         torch.cuda.synchronize()
-    total_ms = ev0.elapsed_time(ev1)
-    if dist:
-        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = reduce_max(ev0.elapsed_time(ev1))
     idx.set_option("stage_timing", 0)
     value = world * nq * args.steps / (total_ms / 1000.0)
 
@@ -228,11 +240,7 @@ def run_ours(args, w, rank, world, local_rank):
         rc = capi.lib().fpp_query(idx.h, Qh.data_ptr(), nq, k, 0, outh.data_ptr())
         if rc != 0:
             raise RuntimeError(capi.lib().fpp_last_error().decode())
-    e2e_s = time.perf_counter() - t0
-    if dist:
-        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = reduce_max(time.perf_counter() - t0)
     e2e = world * nq * args.steps / e2e_s
     assert np.array_equal(outh.numpy(), outd.cpu().numpy()), "host and device query paths disagree"
 

@@ -106,6 +106,7 @@ struct Index {
   int iProbes = 1, qProbes = 1;
   long long seed = -1;
   int fhtDim = 0;
+  int table_lo = 0, table_hi = -1;  // build only tables [lo, hi) when hi >= 0 (tests)
 
   std::vector<float> X;       // centred data, point-major (n x d)
   std::vector<float> center;  // d
@@ -221,6 +222,13 @@ int orc_set_index_param(void* h, int L, int D, int minSize, float alpha, int p, 
 }
 
 void orc_set_qprobes(void* h, int q) { static_cast<Index*>(h)->qProbes = q; }
+
+// Restrict the next build to tables [lo, hi) (the other tables stay empty);
+// used by tests to check a few tables of a large index.
+void orc_set_table_range(void* h, int lo, int hi) {
+  static_cast<Index*>(h)->table_lo = lo;
+  static_cast<Index*>(h)->table_hi = hi;
+}
 void orc_set_threads(void* h, int t) {
   static_cast<Index*>(h)->n_threads = t <= 0 ? omp_get_max_threads() : t;
 }
@@ -252,8 +260,11 @@ long long orc_build(void* h, const float* X) {
   I.bucketRaw.assign((size_t)L * nb, 0);
 
   omp_set_num_threads(I.n_threads);
+  const int lo = I.table_hi >= 0 ? I.table_lo : 0;
+  const int hi = I.table_hi >= 0 ? std::min(I.table_hi, L) : L;
+  for (int l = 0; l < L; ++l) tabCount[l].assign(nb, 0);
 #pragma omp parallel for schedule(dynamic, 1)
-  for (int l = 0; l < L; ++l) {
+  for (int l = lo; l < hi; ++l) {
     std::vector<MaxQue> buckets(nb);
     std::vector<float> v1(I.fhtDim), v2(I.fhtDim);
     std::vector<IFPair> vec1, vec2;
@@ -289,7 +300,6 @@ long long orc_build(void* h, const float* X) {
     }
     std::vector<int>& ids = tabIds[l];
     std::vector<float>& sc = tabScores[l];
-    tabCount[l].assign(nb, 0);
     for (long long b = 0; b < nb; ++b) {  // FalconnPP.cpp:216-266
       if (buckets[b].empty()) continue;
       const int B = (int)buckets[b].size();

@@ -54,6 +54,7 @@ def lib() -> ctypes.CDLL:
             "orc_query_candidates": (i64, [vp, vp, vp, i64]),
             "orc_bf_topk_f64": (None, [vp, i64, i32, vp, i32, i32, i32, vp]),
             "orc_import": (None, [vp, vp, vp, vp, vp, vp, vp, i64]),
+            "orc_set_table_range": (None, [vp, i32, i32]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -133,6 +134,9 @@ class Index:
     def set_qprobes(self, q):
         self.qProbes = q
         lib().orc_set_qprobes(self.h, q)
+
+    def set_table_range(self, lo, hi):
+        lib().orc_set_table_range(self.h, lo, hi)
 
     def set_threads(self, t):
         lib().orc_set_threads(self.h, t)
