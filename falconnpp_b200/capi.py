@@ -19,6 +19,7 @@ EXPORTED = [
     "fpp_build", "fpp_build_device", "fpp_query", "fpp_query_device", "fpp_last_error", "fpp_get_info",
     "fpp_get_stats", "fpp_set_option", "fpp_print_build_report", "fpp_dump_bits", "fpp_dump_center",
     "fpp_dump_tables", "fpp_build_dump_hash", "fpp_query_dump", "fpp_rerank_probes_noalloc",
+    "fpp_set_query_form", "fpp_query_batched",
 ]
 
 _lib = None
@@ -59,6 +60,8 @@ def lib() -> ctypes.CDLL:
             "fpp_build_dump_hash": (i32, [vp, vp, vp, vp]),
             "fpp_query_dump": (i32, [vp, vp, i32, i32, vp, vp, vp, vp, vp, vp, i64]),
             "fpp_rerank_probes_noalloc": (i32, [vp, vp, i32, vp, i32, i32, vp, vp]),
+            "fpp_set_query_form": (i32, [vp, i32, i32, i32]),
+            "fpp_query_batched": (i32, [vp, vp, i32, vp, vp, i32, i32, vp, i32, vp, vp]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -146,6 +149,15 @@ class Index:
         _check(lib().fpp_query_dump(self.h, _ptr(Q), nq, k, _ptr(out), _ptr(val), _ptr(probes), _ptr(pval),
                                     _ptr(stats), _ptr(cands), cand_cap))
         return dict(topk=out, topk_val=val, probes=probes, probe_val=pval, stats=stats, cands=cands)
+
+    def set_query_form(self, form: int, precision: int = 0, shortlist_mult: int = 4):
+        _check(lib().fpp_set_query_form(self.h, form, precision, shortlist_mult))
+
+    def query_batched(self, q_ptr: int, nq: int, k_ptr: int | None, qp_ptr: int | None, k_max: int, qp_max: int,
+                      out_ptr: int, out_stride: int, val_ptr: int | None = None, stream: int | None = None):
+        _check(lib().fpp_query_batched(self.h, ctypes.c_void_p(q_ptr), nq, ctypes.c_void_p(k_ptr or 0),
+                                       ctypes.c_void_p(qp_ptr or 0), k_max, qp_max, ctypes.c_void_p(out_ptr),
+                                       out_stride, ctypes.c_void_p(val_ptr or 0), ctypes.c_void_p(stream or 0)))
 
     def info(self) -> dict:
         v = np.zeros(6, np.int64)

@@ -1,0 +1,851 @@
+// fpp_batch.cu — the batched query form: ONE persistent kernel per batch that
+// runs rotate -> hash -> probe selection -> gather/dedupe -> rerank -> top-k for
+// every query (src/FalconnPP.cpp:345-677 per query), with
+//
+//   * dynamic scheduling: blocks take queries from a work counter, so uneven
+//     qProbes and candidate counts balance across the GPU;
+//   * per-query k and qProbes (arrays), for mixed batches;
+//   * reranking of the candidate rows in BF16 or FP8-E4M3 (per-row FP32 scale)
+//     with FP32 accumulation, then an exact FP32 re-score of a shortlist of
+//     r*k candidates and the top-k of the shortlist; in FP32 mode the kernel
+//     reproduces the plain path bit for bit;
+//   * optional capture of the launch (work-counter reset + kernel) in a CUDA
+//     graph that later calls with the same shape replay.
+//
+// Hashing, probe selection and the tie rules are the plain path's
+// (fpp_query.cu): the hash arithmetic stays FP32 and bit-exact.
+#include <cuda_bf16.h>
+#include <cuda_fp8.h>
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "fpp_batch.h"
+#include "fpp_device.cuh"
+#include "fpp_rows.cuh"
+
+namespace fpp {
+
+constexpr int kBThreads = 256;
+constexpr int kBWarps = kBThreads / 32;
+constexpr int kBMaxList = 2048;   // L * m entries held in shared memory
+constexpr int kBMaxProbes = 1024;
+constexpr int kBMaxM1 = 16;
+constexpr int kBMaxTop = 1024;    // k * shortlist multiple, and the replay heaps
+
+struct BatchArgs {
+  const float* Xc;
+  int ld;
+  const unsigned char* Xrows;  // rows reranked first (fp32 = Xc, else bf16/fp8 copy)
+  size_t row_bytes;
+  int nchunk;
+  const float* Xscale;
+  const uint32_t* flips;
+  const uint32_t* bucket_off;
+  const int32_t* ids;
+  int n, d, L, D, log2D;
+  uint32_t NB;
+  const float* Q;
+  int nq;
+  const int* q_k;
+  const int* q_qprobes;
+  int k_uniform, qprobes_uniform;
+  int k_max, qprobes_max;  // per-query values outside [1, max] are rejected
+  int shortlist_mult;
+  int32_t* out;
+  int out_stride;
+  float* out_v;
+  uint32_t* bitset;
+  long long nwords;
+  uint32_t* uniq;
+  uint32_t* score;
+  long long cap;
+  float* gdump;       // [groups][FHT] fallback dumps
+  float* gheap_v;     // [groups][mmax] pair heaps
+  int* gheap_i;
+  int mmax;
+  unsigned int* work;
+  unsigned int* status;  // bit 0: candidate capacity overflow; bit 1: per-query k/qProbes out of range
+};
+
+__device__ __forceinline__ int ceil_sqrt_int(int m) {
+  int r = 0;
+  while (r * r < m) ++r;
+  return r;
+}
+
+// block-wide radix selection of the `want`-th largest key among n keys
+// produced by key_at(i); returns the key; counts of keys >= it in *ge.
+template <typename F>
+__device__ __forceinline__ uint32_t block_select(int n, unsigned want, F key_at, uint32_t* hist, uint32_t* s_pre,
+                                                 uint32_t* s_rem, unsigned* s_cnt, unsigned* ge_out) {
+  if (threadIdx.x == 0) {
+    *s_pre = 0;
+    *s_rem = want;
+  }
+  uint32_t mask = 0;
+  for (int shift = 24; shift >= 0; shift -= 8) {
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) hist[i] = 0;
+    __syncthreads();
+    const uint32_t pre = *s_pre;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      const uint32_t k = key_at(i);
+      if ((k & mask) == pre) atomicAdd(&hist[(k >> shift) & 255u], 1u);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      uint32_t rem = *s_rem;
+      int dg = 255;
+      for (; dg > 0; --dg) {
+        if (hist[dg] >= rem) break;
+        rem -= hist[dg];
+      }
+      *s_pre = pre | ((uint32_t)dg << shift);
+      *s_rem = rem;
+    }
+    mask |= 255u << shift;
+    __syncthreads();
+  }
+  const uint32_t t = *s_pre;
+  if (threadIdx.x == 0) *s_cnt = 0;
+  __syncthreads();
+  unsigned ge = 0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) ge += key_at(i) >= t;
+  atomicAdd(s_cnt, ge);
+  __syncthreads();
+  *ge_out = *s_cnt;
+  __syncthreads();
+  return t;
+}
+
+// ascending bitonic sort of n (<= kBMaxTop) 64-bit keys in shared memory
+__device__ __forceinline__ void block_sort_u64(unsigned long long* a, int n) {
+  int N = 1;
+  while (N < n) N <<= 1;
+  for (int k2 = 2; k2 <= N; k2 <<= 1)
+    for (int j = k2 >> 1; j > 0; j >>= 1) {
+      for (int t = threadIdx.x; t < N / 2; t += blockDim.x) {
+        const int blk = t / j;
+        int lo, hi;
+        if (j == (k2 >> 1)) {
+          lo = blk * k2 + (t - blk * j);
+          hi = blk * k2 + k2 - 1 - (t - blk * j);
+        } else {
+          lo = blk * 2 * j + (t - blk * j);
+          hi = lo + j;
+        }
+        if (hi < n) {
+          const unsigned long long x = a[lo], y = a[hi];
+          if (x > y) {
+            a[lo] = y;
+            a[hi] = x;
+          }
+        }
+      }
+      __syncthreads();
+    }
+}
+
+// dynamic shared memory of k_batch_query
+template <int GROUPS>
+struct BatchSmem {
+  static constexpr size_t kLv = 0;
+  static constexpr size_t kLb = kLv + 4 * kBMaxList;
+  static constexpr size_t kProbe = kLb + 4 * kBMaxList;
+  static constexpr size_t kTop = kProbe + 4 * kBMaxProbes;
+  static constexpr size_t kHv = kTop + 8 * kBMaxTop;
+  static constexpr size_t kHi = kHv + 4 * kBMaxTop;
+  static constexpr size_t kGv = kHi + 4 * kBMaxTop;
+  static constexpr size_t kGc = kGv + 4 * GROUPS * 2 * (kBMaxM1 + 1);
+  static constexpr size_t kRhv = kGc + 4 * GROUPS * 2 * (kBMaxM1 + 1);
+  static constexpr size_t kRhi = kRhv + 4 * GROUPS * kBMaxM1;
+  static constexpr size_t kQ = kRhi + 4 * GROUPS * kBMaxM1;
+  static constexpr size_t kBytes = kQ + 4 * 1024;
+  float* lv;
+  uint32_t* lb;
+  uint32_t* probe;
+  unsigned long long* top;
+  float* hv;
+  int* hi;
+  float* gv;
+  int* gc;
+  float* rhv;
+  int* rhi;
+  float* q;  // the current query, zero padded to 1024 floats
+  __device__ explicit BatchSmem(unsigned char* p)
+      : lv(reinterpret_cast<float*>(p + kLv)),
+        lb(reinterpret_cast<uint32_t*>(p + kLb)),
+        probe(reinterpret_cast<uint32_t*>(p + kProbe)),
+        top(reinterpret_cast<unsigned long long*>(p + kTop)),
+        hv(reinterpret_cast<float*>(p + kHv)),
+        hi(reinterpret_cast<int*>(p + kHi)),
+        gv(reinterpret_cast<float*>(p + kGv)),
+        gc(reinterpret_cast<int*>(p + kGc)),
+        rhv(reinterpret_cast<float*>(p + kRhv)),
+        rhi(reinterpret_cast<int*>(p + kRhi)),
+        q(reinterpret_cast<float*>(p + kQ)) {}
+};
+
+template <int FHT>
+constexpr size_t batch_smem_bytes() {
+  return BatchSmem<kBThreads / Geo<FHT>::G>::kBytes;
+}
+
+template <int FHT, int MODE, int VI, int VI32>
+__global__ void __launch_bounds__(kBThreads, 2) k_batch_query(BatchArgs a) {
+  constexpr int E = Geo<FHT>::E;
+  constexpr int G = Geo<FHT>::G;
+  constexpr int WORDS = Geo<FHT>::WORDS;
+  constexpr int GROUPS = kBThreads / G;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  BatchSmem<GROUPS> sm(smem_raw);
+  float* s_lv = sm.lv;
+  uint32_t* s_lb = sm.lb;
+  uint32_t* s_probe = sm.probe;
+  unsigned long long* s_top = sm.top;
+  float* s_hv = sm.hv;
+  int* s_hi = sm.hi;
+  __shared__ uint32_t hist[256];
+  __shared__ uint32_t s_pre, s_rem;
+  __shared__ unsigned s_cnt, s_u, s_sel, s_q;
+  __shared__ long long tmp[32];
+
+  const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  const int warp = tid >> 5;
+  const int gl = lane & (G - 1);
+  const int grp = tid / G;
+  const unsigned gmask = (G == 32) ? kFullMask : (((1u << G) - 1u) << (lane & ~(G - 1)));
+  const long long gid = (long long)blockIdx.x * GROUPS + grp;
+  uint32_t* bits = a.bitset + (size_t)blockIdx.x * a.nwords;
+  uint32_t* uq = a.uniq + (size_t)blockIdx.x * a.cap;
+  uint32_t* sc = a.score + (size_t)blockIdx.x * a.cap;
+  float* ydump = a.gdump + gid * FHT;
+  float* ph_v = a.gheap_v + gid * (long long)a.mmax;
+  int* ph_i = a.gheap_i + gid * (long long)a.mmax;
+  const int L = a.L;
+
+  for (;;) {
+    if (tid == 0) s_q = atomicAdd(a.work, 1u);
+    __syncthreads();
+    const unsigned qu = s_q;
+    if (qu >= (unsigned)a.nq) break;
+    const int q = (int)qu;
+    const int k = a.q_k ? a.q_k[q] : a.k_uniform;
+    const int Qp = a.q_qprobes ? a.q_qprobes[q] : a.qprobes_uniform;
+    if (k < 1 || k > a.k_max || Qp < 1 || Qp > a.qprobes_max) {  // block-uniform
+      if (tid == 0) atomicOr(a.status, 2u);
+      for (int j = tid; j < a.out_stride; j += kBThreads) a.out[(size_t)q * a.out_stride + j] = -1;
+      __syncthreads();
+      continue;
+    }
+    const int m = (2 * Qp + L - 1) / L;  // ceil(2.0 * qProbes / L), FalconnPP.cpp:336
+    const int m1 = ceil_sqrt_int(m);     // ceil(sqrt(m)), FalconnPP.cpp:337
+    const int M = L * m;
+    const float* qv = a.Q + (size_t)q * a.d;
+    for (int i = tid; i < 1024; i += kBThreads) sm.q[i] = i < a.d ? qv[i] : 0.0f;
+
+    // ---- 1. rotate + hash every table (FalconnPP.cpp:358-531)
+    {
+      float xr[E];
+#pragma unroll
+      for (int e = 0; e < E; ++e) {
+        const int idx = gl * E + e;
+        xr[e] = idx < a.d ? __ldg(qv + idx) : 0.0f;
+      }
+      const int cnt = min(m1 + 1, a.D);
+      const int rounds = (L + GROUPS - 1) / GROUPS;
+      for (int rd = 0; rd < rounds; ++rd) {
+        const int l = rd * GROUPS + grp;
+        const bool active = l < L;
+        const int lt = active ? l : 0;
+#pragma unroll 1
+        for (int layer = 0; layer < 2; ++layer) {
+          float y[E];
+#pragma unroll
+          for (int e = 0; e < E; ++e) y[e] = xr[e];
+          hd3_rotate<FHT>(y, a.flips + ((size_t)(layer * L + lt) * 3) * WORDS, gl);
+          float* lv = sm.gv + (grp * 2 + layer) * (kBMaxM1 + 1);
+          int* lc = sm.gc + (grp * 2 + layer) * (kBMaxM1 + 1);
+          const int f = group_top_cp_auto<FHT>(y, gl, a.D, a.log2D, cnt, lv, lc);
+          __syncwarp();
+          bool ok = (f == cnt);
+          for (int t = 1; t < cnt; ++t)
+            if (ok && !(lv[t - 1] > lv[t])) ok = false;
+          if (!ok) {
+#pragma unroll
+            for (int e = 0; e < E; ++e) ydump[gl * E + e] = y[e];
+            __syncwarp(gmask);
+            if (gl == 0) replay_layer_topp(ydump, a.D, a.log2D, m1, sm.rhv + grp * kBMaxM1, sm.rhi + grp * kBMaxM1, lv, lc);
+            __syncwarp(gmask);
+          }
+        }
+        if (gl == 0 && active) {
+          const float* lv1 = sm.gv + (grp * 2 + 0) * (kBMaxM1 + 1);
+          const int* lc1 = sm.gc + (grp * 2 + 0) * (kBMaxM1 + 1);
+          const float* lv2 = sm.gv + (grp * 2 + 1) * (kBMaxM1 + 1);
+          const int* lc2 = sm.gc + (grp * 2 + 1) * (kBMaxM1 + 1);
+          const uint32_t tbase = (uint32_t)l * a.NB;
+          const int twoD = 2 * a.D;
+          if (m == 1) {
+            s_lv[l] = __fadd_rn(lv1[0], lv2[0]);
+            s_lb[l] = tbase + (uint32_t)(lc1[0] * twoD + lc2[0]);
+          } else {
+            int hn = 0;
+            for (int i = 0; i < m1; ++i)
+              for (int j = 0; j < m1; ++j)
+                topp_offer<int>(ph_v, ph_i, hn, m, __fadd_rn(lv1[i], lv2[j]), lc1[i] * twoD + lc2[j]);
+            for (int j = m - 1; j >= 0; --j) {
+              s_lv[l * m + j] = ph_v[0];
+              s_lb[l * m + j] = tbase + (uint32_t)ph_i[0];
+              heap_pop<true, int>(ph_v, ph_i, hn);
+            }
+          }
+        }
+        __syncwarp();
+      }
+    }
+    __syncthreads();
+
+    // ---- 2. global top-qProbes of the L*m lists (FalconnPP.cpp:540-582)
+    {
+      unsigned ge;
+      const uint32_t t = block_select(M, (unsigned)Qp, [&](int i) { return ord_key(s_lv[i]); }, hist, &s_pre,
+                                      &s_rem, &s_cnt, &ge);
+      if (ge == (unsigned)Qp) {
+        long long run = 0;
+        for (int base = 0; base < M; base += kBThreads) {
+          const int i = base + tid;
+          const bool take = i < M && ord_key(s_lv[i]) >= t;
+          long long tot;
+          const long long pos = block_exclusive_scan(take ? 1 : 0, tmp, &tot) + run;
+          if (take) s_probe[pos] = s_lb[i];
+          run += tot;
+        }
+      } else if (tid == 0) {
+        int n = 0;
+        int* track = s_hi + L;
+        for (int l = 0; l < L; ++l) {
+          heap_push<false, int>(s_hv, s_hi, n, s_lv[l * m], l * m);
+          track[l] = 0;
+        }
+        for (int pc = 0; pc < Qp; ++pc) {
+          const int pos = s_hi[0];
+          heap_pop<false, int>(s_hv, s_hi, n);
+          s_probe[pc] = s_lb[pos];
+          const int tb = pos / m;
+          track[tb]++;
+          if (track[tb] < m) heap_push<false, int>(s_hv, s_hi, n, s_lv[tb * m + track[tb]], tb * m + track[tb]);
+        }
+      }
+      __syncthreads();
+    }
+
+    // ---- 3. gather + dedupe (FalconnPP.cpp:584-606), the candidates of all
+    // probes flattened over the block's warps, 128 ids per warp step
+    if (tid == 0) s_u = 0;
+    uint32_t* s_po = s_lb;                                // bucket start of probe p
+    uint32_t* s_pe = reinterpret_cast<uint32_t*>(s_lv);  // inclusive end of probe p in the flat range
+    {
+      long long run = 0;
+      for (int base = 0; base < Qp; base += kBThreads) {
+        const int p = base + tid;
+        uint32_t o = 0, sz = 0;
+        if (p < Qp) {
+          const uint32_t g = s_probe[p];
+          o = a.bucket_off[g];
+          sz = a.bucket_off[g + 1] - o;
+        }
+        long long tot;
+        const long long ex = block_exclusive_scan((long long)sz, tmp, &tot) + run;
+        if (p < Qp) {
+          s_po[p] = o;
+          s_pe[p] = (uint32_t)(ex + sz);
+        }
+        run += tot;
+      }
+    }
+    __syncthreads();
+    const uint32_t C = Qp > 0 ? s_pe[Qp - 1] : 0u;
+    const unsigned cap = (unsigned)a.cap;
+    for (uint32_t c0 = (uint32_t)warp * 128u; c0 < C; c0 += kBWarps * 128u) {
+      uint32_t idv[4];
+#pragma unroll
+      for (int h = 0; h < 4; ++h) {
+        const uint32_t i = c0 + h * 32 + lane;
+        idv[h] = 0xffffffffu;
+        if (i < C) {
+          int lo = 0, hi = Qp - 1;  // first probe whose end exceeds i
+          while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (s_pe[mid] > i) hi = mid; else lo = mid + 1;
+          }
+          const uint32_t st = lo > 0 ? s_pe[lo - 1] : 0u;
+          idv[h] = (uint32_t)__ldg(a.ids + s_po[lo] + (i - st));
+        }
+      }
+      bool fresh[4];
+#pragma unroll
+      for (int h = 0; h < 4; ++h) {
+        fresh[h] = false;
+        if (idv[h] != 0xffffffffu) {
+          const uint32_t bit = 1u << (idv[h] & 31u);
+          fresh[h] = (atomicOr(bits + (idv[h] >> 5), bit) & bit) == 0u;
+        }
+      }
+#pragma unroll
+      for (int h = 0; h < 4; ++h) {
+        const unsigned bal = __ballot_sync(kFullMask, fresh[h]);
+        if (bal) {
+          unsigned base = 0;
+          if (lane == 0) base = atomicAdd(&s_u, (unsigned)__popc(bal));
+          base = __shfl_sync(kFullMask, base, 0);
+          const unsigned pos = base + __popc(bal & ((1u << lane) - 1u));
+          if (fresh[h] && pos < cap) uq[pos] = idv[h];
+        }
+      }
+    }
+    __syncthreads();
+    const unsigned U = s_u;
+    int32_t* orow = a.out + (size_t)q * a.out_stride;
+    float* ovrow = a.out_v ? a.out_v + (size_t)q * a.out_stride : nullptr;
+    if (U > cap) {
+      if (tid == 0) atomicOr(a.status, 1u);
+      for (int j = tid; j < k; j += kBThreads) {
+        orow[j] = -1;
+        if (ovrow) ovrow[j] = 0.0f;
+      }
+      for (long long w = tid; w < a.nwords; w += kBThreads) bits[w] = 0u;
+      __syncthreads();
+      continue;
+    }
+
+    // ---- 4. rerank the unique rows (FalconnPP.cpp:642-660)
+    {
+      const float* scl = MODE == kRowsFP8 ? a.Xscale : nullptr;
+      rerank_rows<MODE, VI, (MODE == kRowsF32 ? 2 : 4)>(uq, U, sc, sm.q, a.Xrows, a.row_bytes, a.nchunk, scl,
+                                                           warp, kBWarps, lane);
+    }
+    __syncthreads();
+
+    // ---- 5. shortlist by the first scores, exact FP32 re-score, top-k
+    const unsigned kk = (unsigned)k;
+    const unsigned R = MODE == kRowsF32 ? kk : min((unsigned)kBMaxTop, kk * (unsigned)a.shortlist_mult);
+    unsigned nsel = U;
+    bool exact = true;
+    if (U > R) {
+      unsigned ge;
+      const uint32_t t = block_select((int)U, R, [&](int i) { return ord_key_bits(sc[i]); }, hist, &s_pre, &s_rem,
+                                      &s_cnt, &ge);
+      if (MODE == kRowsF32 && ge != R) {
+        exact = false;  // tie at the k-th score: replay below
+      } else {
+        // keep every entry >= t (ties at the cut included, at most kBMaxTop)
+        if (tid == 0) s_sel = 0;
+        __syncthreads();
+        for (unsigned i = tid; i < U; i += kBThreads) {
+          const uint32_t key = ord_key_bits(sc[i]);
+          if (key >= t) {
+            const unsigned pos = atomicAdd(&s_sel, 1u);
+            if (pos < (unsigned)kBMaxTop) s_top[pos] = ((unsigned long long)(~key) << 32) | uq[i];
+          }
+        }
+        __syncthreads();
+        nsel = min(s_sel, (unsigned)kBMaxTop);
+      }
+    } else {
+      for (unsigned i = tid; i < U; i += kBThreads)
+        s_top[i] = ((unsigned long long)(~ord_key_bits(sc[i])) << 32) | uq[i];
+      __syncthreads();
+    }
+    if (exact && MODE != kRowsF32) {
+      // exact FP32 re-score of the shortlist with the parity dot order
+      __syncthreads();
+      if (nsel > 0) {
+        uint32_t* sid = reinterpret_cast<uint32_t*>(s_hv);  // shortlist ids
+        uint32_t* ssc = reinterpret_cast<uint32_t*>(s_hi);  // their FP32 scores
+        for (unsigned i = tid; i < nsel; i += kBThreads) sid[i] = (uint32_t)s_top[i];
+        __syncthreads();
+        rerank_rows<kRowsF32, VI32>(sid, nsel, ssc, sm.q, reinterpret_cast<const unsigned char*>(a.Xc),
+                                    (size_t)a.ld * 4, a.ld / 4, nullptr, warp, kBWarps, lane);
+        __syncthreads();
+        for (unsigned i = tid; i < nsel; i += kBThreads)
+          s_top[i] = ((unsigned long long)(~ord_key_bits(ssc[i])) << 32) | sid[i];
+        __syncthreads();
+      }
+    }
+    if (exact) {
+      block_sort_u64(s_top, (int)nsel);
+      const unsigned kept = min(nsel, kk);
+      unsigned dup = 0;
+      // equal FP32 scores in the kept list, or at the k-th place: heap order decides
+      for (unsigned i = tid; i + 1 < nsel && i < kk; i += kBThreads) dup |= (s_top[i] >> 32) == (s_top[i + 1] >> 32);
+      exact = !__syncthreads_or(dup);
+      if (exact) {
+        for (int j = tid; j < k; j += kBThreads) {
+          if ((unsigned)j < kept) {
+            orow[j] = (int32_t)(uint32_t)s_top[j];
+            if (ovrow) ovrow[j] = __uint_as_float(ord_key_inv_dev(~(uint32_t)(s_top[j] >> 32)));
+          } else {
+            orow[j] = 0;
+            if (ovrow) ovrow[j] = 0.0f;
+          }
+        }
+      }
+    }
+    if (!exact) {
+      // the reference's min-heap over the candidates in ascending id order
+      // (FalconnPP.cpp:633-673): all of them in FP32 mode, the shortlist otherwise
+      const bool whole = (MODE == kRowsF32);
+      unsigned nc = whole ? U : nsel;
+      uint32_t* cid = uq;
+      uint32_t* csc = sc;
+      if (!whole) {
+        for (unsigned i = tid; i < nc; i += kBThreads) {
+          cid[i] = (uint32_t)s_top[i];
+          csc[i] = ord_key_inv_dev(~(uint32_t)(s_top[i] >> 32));
+        }
+        __syncthreads();
+      }
+      block_bitonic_sort_u32(cid, csc, (int)nc);
+      if (tid == 0) {
+        int n = 0;
+        for (unsigned i = 0; i < nc; ++i) topp_offer<int>(s_hv, s_hi, n, k, __uint_as_float(csc[i]), (int)cid[i]);
+        for (int j = n; j < k; ++j) {
+          orow[j] = 0;
+          if (ovrow) ovrow[j] = 0.0f;
+        }
+        for (int j = n - 1; j >= 0; --j) {
+          orow[j] = s_hi[0];
+          if (ovrow) ovrow[j] = s_hv[0];
+          heap_pop<true, int>(s_hv, s_hi, n);
+        }
+      }
+      __syncthreads();
+      if (!whole) {  // the unique list was overwritten: clear the whole bitset
+        for (long long w = tid; w < a.nwords; w += kBThreads) bits[w] = 0u;
+        __syncthreads();
+        continue;
+      }
+    }
+    __syncthreads();
+    for (unsigned i = tid; i < U; i += kBThreads) bits[uq[i] >> 5] = 0u;
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------- conversion
+__global__ void k_rows_bf16(const float* __restrict__ Xc, long long n, int ld, int ldo, uint16_t* __restrict__ out) {
+  const long long total = n * (long long)ldo;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    const long long i = t / ldo;
+    const int j = (int)(t - i * ldo);
+    const float x = j < ld ? Xc[i * ld + j] : 0.0f;
+    const __nv_bfloat16 b = __float2bfloat16_rn(x);
+    out[t] = *reinterpret_cast<const uint16_t*>(&b);
+  }
+}
+
+// one warp per row: scale = max|x| / 448 (E4M3 largest finite), x8 = x / scale
+__global__ void k_rows_fp8(const float* __restrict__ Xc, long long n, int ld, int ldo, uint8_t* __restrict__ out,
+                           float* __restrict__ scale) {
+  const int lane = threadIdx.x & 31;
+  const long long w = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long i = w; i < n; i += nw) {
+    float mx = 0.0f;
+    for (int j = lane; j < ld; j += 32) mx = fmaxf(mx, fabsf(Xc[i * ld + j]));
+    for (int o = 16; o; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    const float s = mx > 0.0f ? mx / 448.0f : 1.0f;
+    for (int j = lane; j < ldo; j += 32) {
+      const float x = j < ld ? Xc[i * ld + j] / s : 0.0f;
+      out[i * ldo + j] = (uint8_t)__nv_cvt_float_to_fp8(x, __NV_SATFINITE, __NV_E4M3);
+    }
+    if (lane == 0) scale[i] = s;
+  }
+}
+
+// ---------------------------------------------------------------- host side
+int ensure_lowp_rows(const Params& P, DeviceIndex& di, int mode, cudaStream_t s, Error& err) {
+  if (mode == kRowsF32 || di.lp_mode == mode) return kOk;
+  cudaFree(di.Xlp);
+  cudaFree(di.Xlp_scale);
+  di.Xlp = nullptr;
+  di.Xlp_scale = nullptr;
+  di.lp_mode = kRowsF32;
+  const long long n = P.n_points;
+  int dev = 0, nsm = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  cudaError_t e;
+  if (mode == kRowsBF16) {
+    const int ldo = (P.n_features + 7) & ~7;  // 16-byte rows
+    if ((e = cudaMalloc(&di.Xlp, (size_t)n * ldo * 2)) != cudaSuccess) goto fail;
+    k_rows_bf16<<<nsm * 8, 256, 0, s>>>(di.Xc, n, di.ld, ldo, static_cast<uint16_t*>(di.Xlp));
+    di.ld_lp = ldo;
+  } else {
+    const int ldo = (P.n_features + 15) & ~15;
+    if ((e = cudaMalloc(&di.Xlp, (size_t)n * ldo)) != cudaSuccess) goto fail;
+    if ((e = cudaMalloc(&di.Xlp_scale, sizeof(float) * n)) != cudaSuccess) goto fail;
+    k_rows_fp8<<<nsm * 8, 256, 0, s>>>(di.Xc, n, di.ld, ldo, static_cast<uint8_t*>(di.Xlp), di.Xlp_scale);
+    di.ld_lp = ldo;
+  }
+  if ((e = cudaGetLastError()) != cudaSuccess) goto fail;
+  if ((e = cudaStreamSynchronize(s)) != cudaSuccess) goto fail;
+  di.lp_mode = mode;
+  return kOk;
+fail:
+  err.code = (e == cudaErrorMemoryAllocation) ? kErrOutOfMemory : kErrCuda;
+  err.msg = std::string("low-precision rows: ") + cudaGetErrorString(e);
+  cudaFree(di.Xlp);
+  cudaFree(di.Xlp_scale);
+  di.Xlp = nullptr;
+  di.Xlp_scale = nullptr;
+  return err.code;
+}
+
+void BatchWorkspace::release() {
+  if (graph_exec) cudaGraphExecDestroy(graph_exec);
+  cudaFree(bitset);
+  cudaFree(uniq);
+  cudaFree(score);
+  cudaFree(gdump);
+  cudaFree(gheap_v);
+  cudaFree(gheap_i);
+  cudaFree(counters);
+  *this = BatchWorkspace();
+}
+
+struct KernelSel {
+  const void* fn;
+  size_t smem;
+};
+
+template <int FHT, int MODE, int VI, int VI32>
+static KernelSel kernel_ptr() {
+  const void* fn = reinterpret_cast<const void*>(&k_batch_query<FHT, MODE, VI, VI32>);
+  const size_t smem = batch_smem_bytes<FHT>();
+  cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  return KernelSel{fn, smem};
+}
+
+template <int MODE, int VI, int VI32>
+static KernelSel pick_fht(int fht) {
+  switch (fht) {
+    case 2: return kernel_ptr<2, MODE, VI, VI32>();
+    case 4: return kernel_ptr<4, MODE, VI, VI32>();
+    case 8: return kernel_ptr<8, MODE, VI, VI32>();
+    case 16: return kernel_ptr<16, MODE, VI, VI32>();
+    case 32: return kernel_ptr<32, MODE, VI, VI32>();
+    case 64: return kernel_ptr<64, MODE, VI, VI32>();
+    case 128: return kernel_ptr<128, MODE, VI, VI32>();
+    case 256: return kernel_ptr<256, MODE, VI, VI32>();
+    case 512: return kernel_ptr<512, MODE, VI, VI32>();
+    case 1024: return kernel_ptr<1024, MODE, VI, VI32>();
+    default: return KernelSel{nullptr, 0};
+  }
+}
+
+// VI: chunks per virtual lane for the first rerank; VI32: for the FP32 rows.
+static KernelSel pick_kernel(int fht, int mode, int d) {
+  const int vi32 = ((d + 3) / 4 + 31) / 32;  // 1..8
+  if (mode == kRowsF32) {
+    switch (vi32) {
+      case 1: return pick_fht<kRowsF32, 1, 1>(fht);
+      case 2: return pick_fht<kRowsF32, 2, 2>(fht);
+      case 3:
+      case 4: return pick_fht<kRowsF32, 4, 4>(fht);
+      default: return pick_fht<kRowsF32, 8, 8>(fht);
+    }
+  }
+  const int epc = mode == kRowsBF16 ? 8 : 16;
+  const int vi = ((d + epc - 1) / epc + 31) / 32;
+  const int v32 = vi32 <= 1 ? 1 : vi32 <= 2 ? 2 : vi32 <= 4 ? 4 : 8;
+  const int v = vi <= 1 ? 1 : vi <= 2 ? 2 : 4;
+#define FPP_PICK(M, A, B) \
+  if (v == A && v32 == B) return pick_fht<M, A, B>(fht);
+  if (mode == kRowsBF16) {
+    FPP_PICK(kRowsBF16, 1, 1)
+    FPP_PICK(kRowsBF16, 1, 2)
+    FPP_PICK(kRowsBF16, 2, 4)
+    FPP_PICK(kRowsBF16, 4, 8)
+  } else {
+    FPP_PICK(kRowsFP8, 1, 1)
+    FPP_PICK(kRowsFP8, 1, 2)
+    FPP_PICK(kRowsFP8, 1, 4)
+    FPP_PICK(kRowsFP8, 2, 8)
+  }
+#undef FPP_PICK
+  return KernelSel{nullptr, 0};
+}
+
+int batch_query(const Params& P, DeviceIndex& di, BatchWorkspace& bw, const BatchRequest& rq, cudaStream_t s,
+                BatchResult& res, Error& err) {
+  auto fail = [&](cudaError_t e, const char* what) {
+    err.code = (e == cudaErrorMemoryAllocation) ? kErrOutOfMemory : kErrCuda;
+    err.msg = std::string("batch query: ") + what + ": " + cudaGetErrorString(e);
+    return err.code;
+  };
+  res = BatchResult();
+  if (rq.nq <= 0) return kOk;
+  const int L = P.n_tables, D = P.n_proj, d = P.n_features, F = P.fhtDim;
+  const int mmax = (2 * rq.qprobes_max + L - 1) / L;
+  int m1max = 0;
+  while (m1max * m1max < mmax) ++m1max;
+  if (rq.qprobes_max > kBMaxProbes || (long long)L * mmax > kBMaxList || m1max > kBMaxM1 || m1max > D ||
+      L > kBMaxTop / 2) {
+    err.code = kErrUnsupported;
+    err.msg = "batch query: qProbes too large for the batched form (at most 2048 probes, n_tables * probes per "
+              "table <= 4096, ceil(sqrt(probes per table)) <= 16); use the plain form";
+    return err.code;
+  }
+  if (rq.k_max < 1 || (long long)rq.k_max * (rq.mode == kRowsF32 ? 1 : rq.shortlist_mult) > kBMaxTop) {
+    err.code = kErrInvalidArgument;
+    err.msg = "batch query: k * shortlist multiple must be <= 1024";
+    return err.code;
+  }
+  if (rq.mode != kRowsF32) {
+    const int rc = ensure_lowp_rows(P, di, rq.mode, s, err);
+    if (rc) return rc;
+  }
+  const KernelSel ks = pick_kernel(F, rq.mode, d);
+  const void* kern = ks.fn;
+  if (!kern) {
+    err.code = kErrUnsupported;
+    err.msg = "batch query: no kernel for this shape";
+    return err.code;
+  }
+  int dev = 0, nsm = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  cudaError_t e;
+  int per_sm = 0;
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kBThreads, ks.smem)) != cudaSuccess)
+    return fail(e, "occupancy");
+  if (rq.blocks_per_sm > 0) per_sm = std::min(per_sm, rq.blocks_per_sm);
+  per_sm = std::max(per_sm, 1);
+  int grid = std::max(1, std::min(rq.nq, nsm * per_sm));
+  const long long nwords = (P.n_points + 31) / 32;
+  const long long cap = std::max<long long>(
+      1, std::min<long long>(P.n_points, (long long)rq.qprobes_max * std::max<uint32_t>(di.max_kept, 1u)));
+  const int groups = grid * (kBThreads / (F < 32 ? 1 : F / 32));
+  // (re)allocate per-block scratch when the shape grows
+  if (!bw.bitset || bw.grid < grid || bw.nwords != nwords || bw.cap < cap || bw.fht < F || bw.mmax < mmax) {
+    bw.release();
+    if ((e = cudaMalloc(&bw.bitset, sizeof(uint32_t) * (size_t)grid * nwords)) != cudaSuccess) return fail(e, "alloc");
+    if ((e = cudaMemsetAsync(bw.bitset, 0, sizeof(uint32_t) * (size_t)grid * nwords, s)) != cudaSuccess)
+      return fail(e, "memset");
+    if ((e = cudaMalloc(&bw.uniq, sizeof(uint32_t) * (size_t)grid * cap)) != cudaSuccess) return fail(e, "alloc");
+    if ((e = cudaMalloc(&bw.score, sizeof(uint32_t) * (size_t)grid * cap)) != cudaSuccess) return fail(e, "alloc");
+    if ((e = cudaMalloc(&bw.gdump, sizeof(float) * (size_t)groups * F)) != cudaSuccess) return fail(e, "alloc");
+    if ((e = cudaMalloc(&bw.gheap_v, sizeof(float) * (size_t)groups * std::max(mmax, 1))) != cudaSuccess)
+      return fail(e, "alloc");
+    if ((e = cudaMalloc(&bw.gheap_i, sizeof(int) * (size_t)groups * std::max(mmax, 1))) != cudaSuccess)
+      return fail(e, "alloc");
+    if ((e = cudaMalloc(&bw.counters, sizeof(unsigned) * 4)) != cudaSuccess) return fail(e, "alloc");
+    bw.grid = grid;
+    bw.nwords = nwords;
+    bw.cap = cap;
+    bw.fht = F;
+    bw.mmax = std::max(mmax, 1);
+  }
+  grid = std::min(grid, bw.grid);
+  BatchArgs a;
+  a.Xc = di.Xc;
+  a.ld = di.ld;
+  if (rq.mode == kRowsF32) {
+    a.Xrows = reinterpret_cast<const unsigned char*>(di.Xc);
+    a.row_bytes = (size_t)di.ld * 4;
+    a.nchunk = di.ld / 4;
+  } else if (rq.mode == kRowsBF16) {
+    a.Xrows = static_cast<const unsigned char*>(di.Xlp);
+    a.row_bytes = (size_t)di.ld_lp * 2;
+    a.nchunk = di.ld_lp / 8;
+  } else {
+    a.Xrows = static_cast<const unsigned char*>(di.Xlp);
+    a.row_bytes = (size_t)di.ld_lp;
+    a.nchunk = di.ld_lp / 16;
+  }
+  a.Xscale = di.Xlp_scale;
+  a.flips = di.flips;
+  a.bucket_off = di.bucket_off;
+  a.ids = di.ids;
+  a.n = P.n_points;
+  a.d = d;
+  a.L = L;
+  a.D = D;
+  int log2D = 0;
+  while ((1 << log2D) < D) ++log2D;
+  a.log2D = log2D;
+  a.NB = 4u * (uint32_t)D * (uint32_t)D;
+  a.Q = rq.Q;
+  a.nq = rq.nq;
+  a.q_k = rq.q_k;
+  a.q_qprobes = rq.q_qprobes;
+  a.k_uniform = rq.k_uniform;
+  a.qprobes_uniform = rq.qprobes_uniform;
+  a.k_max = rq.k_max;
+  a.qprobes_max = rq.qprobes_max;
+  a.shortlist_mult = rq.shortlist_mult;
+  a.out = rq.out;
+  a.out_stride = rq.out_stride;
+  a.out_v = rq.out_v;
+  a.bitset = bw.bitset;
+  a.nwords = bw.nwords;
+  a.uniq = bw.uniq;
+  a.score = bw.score;
+  a.cap = bw.cap;
+  a.gdump = bw.gdump;
+  a.gheap_v = bw.gheap_v;
+  a.gheap_i = bw.gheap_i;
+  a.mmax = bw.mmax;
+  a.work = bw.counters;
+  a.status = bw.counters + 1;
+  void* args[] = {&a};
+
+  const bool can_graph = rq.use_graph;
+  BatchKey key{rq.Q, rq.nq, rq.q_k, rq.q_qprobes, rq.k_uniform, rq.qprobes_uniform, rq.k_max, rq.qprobes_max,
+               rq.shortlist_mult, rq.out,
+               rq.out_stride, rq.out_v, rq.mode, grid, kern, bw.bitset, s};
+  if (can_graph && bw.graph_exec && bw.key == key) {
+    if ((e = cudaGraphLaunch(bw.graph_exec, s)) != cudaSuccess) return fail(e, "graph launch");
+    res.graph_replayed = true;
+  } else {
+    if (can_graph) {
+      if (bw.graph_exec) {
+        cudaGraphExecDestroy(bw.graph_exec);
+        bw.graph_exec = nullptr;
+      }
+      cudaGraph_t graph = nullptr;
+      if ((e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) return fail(e, "capture");
+      cudaMemsetAsync(bw.counters, 0, sizeof(unsigned) * 2, s);
+      cudaLaunchKernel(kern, dim3(grid), dim3(kBThreads), args, ks.smem, s);
+      if ((e = cudaStreamEndCapture(s, &graph)) != cudaSuccess) return fail(e, "capture end");
+      e = cudaGraphInstantiate(&bw.graph_exec, graph, 0);
+      cudaGraphDestroy(graph);
+      if (e != cudaSuccess) return fail(e, "graph instantiate");
+      bw.key = key;
+      if ((e = cudaGraphLaunch(bw.graph_exec, s)) != cudaSuccess) return fail(e, "graph launch");
+    } else {
+      if ((e = cudaMemsetAsync(bw.counters, 0, sizeof(unsigned) * 2, s)) != cudaSuccess) return fail(e, "memset");
+      if ((e = cudaLaunchKernel(kern, dim3(grid), dim3(kBThreads), args, ks.smem, s)) != cudaSuccess)
+        return fail(e, "launch");
+    }
+  }
+  res.launches = 1;
+  res.grid = grid;
+  if (rq.check_status) {
+    unsigned st[2] = {0, 0};
+    if ((e = cudaMemcpyAsync(st, bw.counters, sizeof(st), cudaMemcpyDeviceToHost, s)) != cudaSuccess)
+      return fail(e, "status");
+    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return fail(e, "batch kernel");
+    res.overflow = (st[1] & 1u) != 0;
+    res.bad_params = (st[1] & 2u) != 0;
+  }
+  return kOk;
+}
+
+}  // namespace fpp

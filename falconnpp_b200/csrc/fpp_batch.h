@@ -1,0 +1,80 @@
+// fpp_batch.h — the batched query form (one persistent fused kernel per batch).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "fpp_index.h"
+
+namespace fpp {
+
+struct BatchRequest {
+  const float* Q = nullptr;  // device, nq x d
+  int nq = 0;
+  const int* q_k = nullptr;        // device per-query k (nullable -> k_uniform)
+  const int* q_qprobes = nullptr;  // device per-query qProbes (nullable -> qprobes_uniform)
+  int k_uniform = 0, qprobes_uniform = 0;
+  int k_max = 0, qprobes_max = 0;  // bounds over the batch (scratch sizing)
+  int mode = 0;                    // RowMode: 0 fp32 (exact), 1 bf16, 2 fp8
+  int shortlist_mult = 4;          // FP32 re-score of shortlist_mult * k candidates
+  int32_t* out = nullptr;          // device, nq x out_stride
+  int out_stride = 0;
+  float* out_v = nullptr;          // optional scores
+  bool use_graph = false;
+  bool check_status = true;        // synchronise and report overflow
+  int blocks_per_sm = 0;           // 0 = as many as fit
+};
+
+struct BatchResult {
+  int launches = 0;
+  int grid = 0;
+  bool graph_replayed = false;
+  bool overflow = false;
+  bool bad_params = false;
+};
+
+struct BatchKey {
+  const float* Q;
+  int nq;
+  const int* q_k;
+  const int* q_qprobes;
+  int k_uniform, qprobes_uniform, k_max, qprobes_max, shortlist_mult;
+  int32_t* out;
+  int out_stride;
+  float* out_v;
+  int mode, grid;
+  const void* kern;
+  uint32_t* bitset;
+  cudaStream_t stream;
+  bool operator==(const BatchKey& o) const {
+    return Q == o.Q && nq == o.nq && q_k == o.q_k && q_qprobes == o.q_qprobes && k_uniform == o.k_uniform &&
+           qprobes_uniform == o.qprobes_uniform && k_max == o.k_max && qprobes_max == o.qprobes_max && shortlist_mult == o.shortlist_mult && out == o.out &&
+           out_stride == o.out_stride && out_v == o.out_v && mode == o.mode && grid == o.grid && kern == o.kern &&
+           bitset == o.bitset && stream == o.stream;
+  }
+};
+
+// Per-block scratch of the batched kernel (kept between calls) and the cached graph.
+struct BatchWorkspace {
+  uint32_t* bitset = nullptr;
+  long long nwords = 0;
+  uint32_t* uniq = nullptr;
+  uint32_t* score = nullptr;
+  long long cap = 0;
+  float* gdump = nullptr;
+  float* gheap_v = nullptr;
+  int* gheap_i = nullptr;
+  int mmax = 0;
+  int fht = 0;
+  int grid = 0;
+  unsigned* counters = nullptr;
+  cudaGraphExec_t graph_exec = nullptr;
+  BatchKey key{};
+  void release();
+};
+
+int ensure_lowp_rows(const Params& P, DeviceIndex& di, int mode, cudaStream_t s, Error& err);
+
+int batch_query(const Params& P, DeviceIndex& di, BatchWorkspace& bw, const BatchRequest& rq, cudaStream_t s,
+                BatchResult& res, Error& err);
+
+}  // namespace fpp

@@ -115,7 +115,7 @@ struct HashSmem {
 
 // Block = 128 threads; a group of G lanes per point; grid-stride over points.
 template <int FHT>
-__global__ void __launch_bounds__(128) k_build_hash(HashArgs a) {
+__global__ void __launch_bounds__(128, 4) k_build_hash(HashArgs a) {
   constexpr int E = Geo<FHT>::E;
   constexpr int G = Geo<FHT>::G;
   constexpr int WORDS = Geo<FHT>::WORDS;
@@ -149,35 +149,26 @@ __global__ void __launch_bounds__(128) k_build_hash(HashArgs a) {
       xr[e] = (active && idx < a.d) ? __ldg(a.Xc + (size_t)pt * a.ld + idx) : 0.0f;
     }
     for (int l = a.l0; l < a.l1; ++l) {
-      float y1[E], y2[E];
+#pragma unroll 1
+      for (int layer = 0; layer < 2; ++layer) {
+        float y[E];
 #pragma unroll
-      for (int e = 0; e < E; ++e) {
-        y1[e] = xr[e];
-        y2[e] = xr[e];
-      }
-      hd3_rotate<FHT>(y1, a.flips + ((size_t)(0 * a.L + l) * 3) * WORDS, gl);
-      hd3_rotate<FHT>(y2, a.flips + ((size_t)(1 * a.L + l) * 3) * WORDS, gl);
-      const int f1 = group_top_cp<FHT>(y1, gl, a.D, a.log2D, cnt, lv1, lc1);
-      const int f2 = group_top_cp<FHT>(y2, gl, a.D, a.log2D, cnt, lv2, lc2);
-      __syncwarp();
-      bool ok1 = (f1 == cnt), ok2 = (f2 == cnt);
-      for (int t = 1; t < cnt; ++t) {
-        if (ok1 && !(lv1[t - 1] > lv1[t])) ok1 = false;
-        if (ok2 && !(lv2[t - 1] > lv2[t])) ok2 = false;
-      }
-      if (!ok1) {  // group-uniform: replay the reference's heap scan
+        for (int e = 0; e < E; ++e) y[e] = xr[e];
+        hd3_rotate<FHT>(y, a.flips + ((size_t)(layer * a.L + l) * 3) * WORDS, gl);
+        float* lv = layer == 0 ? lv1 : lv2;
+        int* lc = layer == 0 ? lc1 : lc2;
+        const int f = group_top_cp_auto<FHT>(y, gl, a.D, a.log2D, cnt, lv, lc);
+        __syncwarp();
+        bool ok = (f == cnt);
+        for (int t = 1; t < cnt; ++t)
+          if (ok && !(lv[t - 1] > lv[t])) ok = false;
+        if (!ok) {  // group-uniform: replay the reference's heap scan
 #pragma unroll
-        for (int e = 0; e < E; ++e) ydump[gl * E + e] = y1[e];
-        __syncwarp(gmask);
-        if (gl == 0) replay_layer_topp(ydump, a.D, a.log2D, P, hv, hi, lv1, lc1);
-        __syncwarp(gmask);
-      }
-      if (!ok2) {
-#pragma unroll
-        for (int e = 0; e < E; ++e) ydump[gl * E + e] = y2[e];
-        __syncwarp(gmask);
-        if (gl == 0) replay_layer_topp(ydump, a.D, a.log2D, P, hv, hi, lv2, lc2);
-        __syncwarp(gmask);
+          for (int e = 0; e < E; ++e) ydump[gl * E + e] = y[e];
+          __syncwarp(gmask);
+          if (gl == 0) replay_layer_topp(ydump, a.D, a.log2D, P, hv, hi, lv, lc);
+          __syncwarp(gmask);
+        }
       }
       if (gl == 0 && active) {
         // two-layer combination, FalconnPP.cpp:162-189 (always replayed: P^2 offers)
@@ -496,7 +487,7 @@ __global__ void __launch_bounds__(256) k_repair(RepairArgs a) {
     uint32_t* psc = in_smem ? s_sc : a.sv + s0;
     for (uint32_t i = threadIdx.x; i < B; i += blockDim.x) {
       pid[i] = a.vals[s0 + i];
-      psc[i] = __float_as_uint(ord_key_inv_dev(~(uint32_t)a.keys[s0 + i]));
+      psc[i] = ord_key_inv_dev(~(uint32_t)a.keys[s0 + i]);  // float bits of the score
     }
     __syncthreads();
     block_bitonic_sort_u32(pid, psc, (int)B);

@@ -101,6 +101,7 @@ int do_build(fpp_index* h, const float* X, bool on_device, cudaStream_t s, int32
     }
   }
   h->ws.release();
+  h->bw.release();
   h->built = false;
   fpp::Error err{0, ""};
   h->bst = fpp::BuildStats();
@@ -138,6 +139,33 @@ void print_build(const fpp_index* h) {
   std::cout << "Percentage of scaled buckets in a table: " << 1.0 * h->bst.n_limited / nb << std::endl;
   std::cout << "Construct Falconn++ (2 layers) Wall Time (in seconds): " << (float)(int)(h->bst.ms_total / 1000.0)
             << " seconds" << std::endl;
+}
+
+// Runs the batched form for device queries/outputs (uniform k, the handle's qProbes).
+int run_batched(fpp_index* h, const float* dQ, int nq, int k, int32_t* dout, cudaStream_t s) {
+  fpp::BatchRequest rq;
+  rq.Q = dQ;
+  rq.nq = nq;
+  rq.k_uniform = k;
+  rq.qprobes_uniform = h->P.qProbes;
+  rq.k_max = k;
+  rq.qprobes_max = h->P.qProbes;
+  rq.mode = h->precision;
+  rq.shortlist_mult = h->shortlist_mult;
+  rq.out = dout;
+  rq.out_stride = k;
+  rq.use_graph = h->use_graph;
+  rq.blocks_per_sm = h->blocks_per_sm;
+  rq.check_status = true;
+  fpp::BatchResult res;
+  fpp::Error err{0, ""};
+  const int rc = fpp::batch_query(h->P, h->di, h->bw, rq, s, res, err);
+  if (rc) return fail(rc, err.msg);
+  if (res.overflow) return fail(FPP_ERR_UNSUPPORTED, "batched query: candidate capacity exceeded");
+  h->qst = fpp::QueryStats();
+  h->qst.launches = res.launches;
+  h->qst.total_probes = (long long)nq * h->P.qProbes;
+  return FPP_OK;
 }
 
 }  // namespace
@@ -180,6 +208,7 @@ void fpp_destroy(fpp_index* h) {
     std::lock_guard<std::mutex> g(h->mu);
     cudaSetDevice(h->device);
     h->ws.release();
+    h->bw.release();
     fpp::free_index(h->di);
     if (h->stream) cudaStreamDestroy(h->stream);
   }
@@ -235,6 +264,7 @@ int fpp_clear(fpp_index* h) {
   std::lock_guard<std::mutex> g(h->mu);
   cudaSetDevice(h->device);
   h->ws.release();
+  h->bw.release();
   fpp::free_index(h->di);
   h->bits = fpp::HostBits();
   h->built = false;
@@ -246,6 +276,11 @@ int fpp_set_option(fpp_index* h, const char* key, long long value) {
   std::lock_guard<std::mutex> g(h->mu);
   if (!strcmp(key, "exact_bucket_order")) {
     h->opt.exact_bucket_order = value != 0;
+  } else if (!strcmp(key, "use_graph")) {
+    h->use_graph = value != 0;
+  } else if (!strcmp(key, "blocks_per_sm")) {
+    if (value < 0) return fail(FPP_ERR_INVALID_ARGUMENT, "set_option: blocks_per_sm must be >= 0");
+    h->blocks_per_sm = (int)value;
   } else if (!strcmp(key, "stage_timing")) {
     h->ws.stage_timing = value != 0;
   } else if (!strcmp(key, "tables_per_chunk")) {
@@ -292,9 +327,36 @@ int fpp_query(fpp_index* h, const float* queries, int n_queries, int n_neighbors
   }
   const auto t0 = std::chrono::high_resolution_clock::now();
   fpp::Error err{0, ""};
-  rc = fpp::query_index(P, h->di, queries, false, n_queries, n_neighbors, out, false, h->ws, h->qst, h->stream, err,
-                        nullptr);
-  if (rc) return fail(rc, err.msg);
+  if (h->form == 1 && n_queries > 0) {
+    // batched form: stage the queries and results through the workspace
+    size_t capq = h->ws.cap_Qd, capo = h->ws.cap_out;
+    cudaError_t e = cudaSuccess;
+    if ((size_t)n_queries * P.n_features > capq) {
+      cudaFree(h->ws.Qd);
+      h->ws.Qd = nullptr;
+      h->ws.cap_Qd = 0;
+      e = cudaMalloc(&h->ws.Qd, sizeof(float) * n_queries * P.n_features);
+      if (e == cudaSuccess) h->ws.cap_Qd = (size_t)n_queries * P.n_features;
+    }
+    if (e == cudaSuccess && (size_t)n_queries * n_neighbors > capo) {
+      cudaFree(h->ws.out);
+      h->ws.out = nullptr;
+      h->ws.cap_out = 0;
+      e = cudaMalloc(&h->ws.out, sizeof(int32_t) * n_queries * n_neighbors);
+      if (e == cudaSuccess) h->ws.cap_out = (size_t)n_queries * n_neighbors;
+    }
+    if (e != cudaSuccess) return fail(FPP_ERR_OUT_OF_MEMORY, std::string("query: ") + cudaGetErrorString(e));
+    cudaMemcpyAsync(h->ws.Qd, queries, sizeof(float) * n_queries * P.n_features, cudaMemcpyHostToDevice, h->stream);
+    rc = run_batched(h, h->ws.Qd, n_queries, n_neighbors, h->ws.out, h->stream);
+    if (rc) return rc;
+    e = cudaMemcpyAsync(out, h->ws.out, sizeof(int32_t) * n_queries * n_neighbors, cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) return fail(FPP_ERR_CUDA, std::string("query: ") + cudaGetErrorString(e));
+  } else {
+    rc = fpp::query_index(P, h->di, queries, false, n_queries, n_neighbors, out, false, h->ws, h->qst, h->stream,
+                          err, nullptr);
+    if (rc) return fail(rc, err.msg);
+  }
   if (verbose && n_queries > 0) {
     const auto ms = std::chrono::duration_cast<std::chrono::milliseconds>(std::chrono::high_resolution_clock::now() - t0);
     const fpp::QueryStats& s = h->qst;
@@ -326,9 +388,70 @@ int fpp_query_device(fpp_index* h, const float* d_queries, int n_queries, int n_
   if (use_device(h)) return FPP_ERR_CUDA;
   cudaStream_t s = stream ? (cudaStream_t)stream : h->stream;
   fpp::Error err{0, ""};
+  if (h->form == 1) {
+    rc = run_batched(h, d_queries, n_queries, n_neighbors, d_out, s);
+    if (rc) return rc;
+    return ok();
+  }
   rc = fpp::query_index(h->P, h->di, d_queries, true, n_queries, n_neighbors, d_out, true, h->ws, h->qst, s, err,
                         nullptr);
   if (rc) return fail(rc, err.msg);
+  return ok();
+}
+
+int fpp_set_query_form(fpp_index* h, int form, int precision, int shortlist_mult) {
+  if (!h) return fail(FPP_ERR_INVALID_ARGUMENT, "set_query_form: NULL handle");
+  if (form < 0 || form > 1) return fail(FPP_ERR_INVALID_ARGUMENT, "set_query_form: form must be 0 or 1");
+  if (precision < 0 || precision > 2) return fail(FPP_ERR_INVALID_ARGUMENT, "set_query_form: precision must be 0..2");
+  if (shortlist_mult < 1 || shortlist_mult > 64)
+    return fail(FPP_ERR_INVALID_ARGUMENT, "set_query_form: shortlist_mult must be in [1, 64]");
+  if (form == 0 && precision != 0)
+    return fail(FPP_ERR_INVALID_ARGUMENT, "set_query_form: the plain form is FP32 only");
+  std::lock_guard<std::mutex> g(h->mu);
+  h->form = form;
+  h->precision = precision;
+  h->shortlist_mult = shortlist_mult;
+  return ok();
+}
+
+int fpp_query_batched(fpp_index* h, const float* d_queries, int n_queries, const int32_t* d_k,
+                      const int32_t* d_qprobes, int k_max, int qprobes_max, int32_t* d_out, int out_stride,
+                      float* d_out_val, void* stream) {
+  if (!h) return fail(FPP_ERR_INVALID_ARGUMENT, "query_batched: NULL handle");
+  std::lock_guard<std::mutex> g(h->mu);
+  if (!h->built) return fail(FPP_ERR_NOT_BUILT, "query_batched: the index is not built");
+  if (n_queries < 0 || k_max < 1 || k_max > 1024 || qprobes_max < 1 || out_stride < k_max)
+    return fail(FPP_ERR_INVALID_ARGUMENT, "query_batched: bad sizes (need 1 <= k <= 1024, out_stride >= k_max)");
+  if (n_queries == 0) return ok();
+  if (!d_queries || !d_out) return fail(FPP_ERR_INVALID_ARGUMENT, "query_batched: NULL buffer");
+  if (use_device(h)) return FPP_ERR_CUDA;
+  cudaStream_t s = stream ? (cudaStream_t)stream : h->stream;
+  fpp::BatchRequest rq;
+  rq.Q = d_queries;
+  rq.nq = n_queries;
+  rq.q_k = d_k;
+  rq.q_qprobes = d_qprobes;
+  rq.k_uniform = k_max;
+  rq.qprobes_uniform = qprobes_max;
+  rq.k_max = k_max;
+  rq.qprobes_max = qprobes_max;
+  rq.mode = h->precision;
+  rq.shortlist_mult = h->shortlist_mult;
+  rq.out = d_out;
+  rq.out_stride = out_stride;
+  rq.out_v = d_out_val;
+  rq.use_graph = h->use_graph;
+  rq.blocks_per_sm = h->blocks_per_sm;
+  rq.check_status = true;
+  fpp::BatchResult res;
+  fpp::Error err{0, ""};
+  const int rc = fpp::batch_query(h->P, h->di, h->bw, rq, s, res, err);
+  if (rc) return fail(rc, err.msg);
+  if (res.overflow) return fail(FPP_ERR_UNSUPPORTED, "query_batched: candidate capacity exceeded");
+  if (res.bad_params)
+    return fail(FPP_ERR_INVALID_ARGUMENT, "query_batched: a per-query k or qProbes is outside [1, k_max/qprobes_max]");
+  h->qst = fpp::QueryStats();
+  h->qst.launches = res.launches;
   return ok();
 }
 

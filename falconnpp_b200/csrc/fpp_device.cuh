@@ -50,13 +50,17 @@ __device__ __forceinline__ void fwht_group(float (&y)[Geo<FHT>::E], int gl) {
       }
     }
   }
+  // Cross-lane stages: the lower lane needs y + o, the upper lane o - y.  Both
+  // are fma(sgn, y, o) with sgn = +1 / -1: the product is exact, so the single
+  // rounding of the fma equals the rounding of the add or subtract (zeros
+  // included: -0 + -0 = -0 and -0 - -0 = +0 either way).
 #pragma unroll
   for (int s = 1; s < G; s <<= 1) {
-    const bool upper = (gl & s) != 0;
+    const float sgn = (gl & s) ? -1.0f : 1.0f;
 #pragma unroll
     for (int e = 0; e < E; ++e) {
       const float o = __shfl_xor_sync(kFullMask, y[e], s);
-      y[e] = upper ? __fsub_rn(o, y[e]) : __fadd_rn(y[e], o);
+      y[e] = __fmaf_rn(sgn, y[e], o);
     }
   }
 }
@@ -146,6 +150,94 @@ __device__ __forceinline__ int group_top_cp(const float (&y)[Geo<FHT>::E], int g
     ++found;
   }
   return found;
+}
+
+// Same result as group_top_cp for cnt <= K: one pass builds each lane's
+// top-K (value desc, position asc), then cnt merge rounds take the group's
+// best head (a lane can win at most cnt times, so K entries per lane suffice).
+template <int FHT, int K>
+__device__ __forceinline__ int group_top_cp_small(const float (&y)[Geo<FHT>::E], int gl, int D, int log2D,
+                                                  int cnt, float* out_v, int* out_c) {
+  constexpr int E = Geo<FHT>::E;
+  constexpr int G = Geo<FHT>::G;
+  float bv[K];
+  int br[K], bc[K];
+#pragma unroll
+  for (int i = 0; i < K; ++i) {
+    bv[i] = -1.0f;
+    br[i] = 0x7fffffff;
+    bc[i] = 0;
+  }
+#pragma unroll
+  for (int e = 0; e < E; ++e) {
+    const int r = gl * E + e;
+    const float v = cp_value(y[e]);
+    // positions rise within the lane, so a strictly larger value is required
+    // to move ahead: equal values keep the earlier position first
+    if (r < D && v > bv[K - 1]) {
+      bv[K - 1] = v;
+      br[K - 1] = r;
+      bc[K - 1] = cp_code(y[e], r, log2D);
+#pragma unroll
+      for (int i = K - 1; i > 0; --i) {
+        if (bv[i] > bv[i - 1]) {
+          const float tv = bv[i];
+          bv[i] = bv[i - 1];
+          bv[i - 1] = tv;
+          const int tr = br[i];
+          br[i] = br[i - 1];
+          br[i - 1] = tr;
+          const int tc = bc[i];
+          bc[i] = bc[i - 1];
+          bc[i - 1] = tc;
+        }
+      }
+    }
+  }
+  int head = 0, found = 0;
+  for (int t = 0; t < cnt; ++t) {
+    float hv = -1.0f;
+    int hr = 0x7fffffff, hc = 0;
+#pragma unroll
+    for (int i = 0; i < K; ++i)
+      if (i == head) {
+        hv = bv[i];
+        hr = br[i];
+        hc = bc[i];
+      }
+    float wv = hv;
+    int wr = hr;
+#pragma unroll
+    for (int s = 1; s < G; s <<= 1) {
+      const float ov = __shfl_xor_sync(kFullMask, wv, s);
+      const int orr = __shfl_xor_sync(kFullMask, wr, s);
+      if (cp_better(ov, orr, wv, wr)) {
+        wv = ov;
+        wr = orr;
+      }
+    }
+    if (wr == 0x7fffffff) break;
+    const bool mine = (wr == hr);
+    const int owner = (threadIdx.x & 31 & ~(G - 1)) + wr / E;
+    const int code = __shfl_sync(kFullMask, hc, owner);
+    if (mine) ++head;
+    if (gl == 0) {
+      out_v[t] = wv;
+      out_c[t] = code;
+    }
+    ++found;
+  }
+  return found;
+}
+
+// Dispatch: the single-pass selection when cnt is small, the round-based one
+// otherwise.
+template <int FHT>
+__device__ __forceinline__ int group_top_cp_auto(const float (&y)[Geo<FHT>::E], int gl, int D, int log2D, int cnt,
+                                                 float* out_v, int* out_c) {
+  if (cnt <= 2) return group_top_cp_small<FHT, 2>(y, gl, D, log2D, cnt, out_v, out_c);
+  if (cnt <= 4) return group_top_cp_small<FHT, 4>(y, gl, D, log2D, cnt, out_v, out_c);
+  return group_top_cp<FHT>(y, gl, D, log2D, cnt, out_v, out_c);
 }
 
 // Exact replay of the reference's per-layer top-p scan (FalconnPP.cpp:103-156,

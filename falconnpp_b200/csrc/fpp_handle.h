@@ -5,6 +5,7 @@
 #include <mutex>
 #include <string>
 
+#include "fpp_batch.h"
 #include "fpp_index.h"
 #include "fpp_query.h"
 
@@ -16,6 +17,12 @@ struct fpp_index {
   fpp::BuildOptions opt;
   fpp::BuildStats bst;
   fpp::QueryStats qst;
+  fpp::BatchWorkspace bw;
+  int form = 0;             // 0 plain three-kernel path, 1 batched fused kernel
+  int precision = 0;        // batched form: 0 FP32 (exact), 1 BF16, 2 FP8-E4M3
+  int shortlist_mult = 4;   // batched low precision: FP32 re-score of shortlist_mult * k
+  bool use_graph = false;   // batched form: capture/replay the launch as a CUDA graph
+  int blocks_per_sm = 0;    // batched form: 0 = occupancy limit
   bool params_set = false;
   bool built = false;
   int device = 0;

@@ -30,7 +30,6 @@
 namespace fpp {
 
 constexpr int kMaxM1 = 64;        // per-layer probes kept per table
-constexpr int kMaxM = 4096;       // probes per table (m1^2)
 
 // ------------------------------------------------------------ query hashing
 struct QHashArgs {
@@ -53,7 +52,7 @@ struct QHashSmem {
 };
 
 template <int FHT>
-__global__ void __launch_bounds__(128) k_query_hash(QHashArgs a, float* heap_v, int* heap_i) {
+__global__ void __launch_bounds__(128, 4) k_query_hash(QHashArgs a, float* heap_v, int* heap_i) {
   constexpr int E = Geo<FHT>::E;
   constexpr int G = Geo<FHT>::G;
   constexpr int WORDS = Geo<FHT>::WORDS;
@@ -87,37 +86,32 @@ __global__ void __launch_bounds__(128) k_query_hash(QHashArgs a, float* heap_v, 
     const long long itm = active ? item : 0;
     const int q = (int)(itm / a.L);
     const int l = (int)(itm - (long long)q * a.L);
-    float y1[E], y2[E];
+    float xr[E];
 #pragma unroll
     for (int e = 0; e < E; ++e) {
       const int idx = gl * E + e;
-      const float x = (active && idx < a.d) ? __ldg(a.Q + (size_t)q * a.d + idx) : 0.0f;
-      y1[e] = x;
-      y2[e] = x;
+      xr[e] = (active && idx < a.d) ? __ldg(a.Q + (size_t)q * a.d + idx) : 0.0f;
     }
-    hd3_rotate<FHT>(y1, a.flips + ((size_t)(0 * a.L + l) * 3) * WORDS, gl);
-    hd3_rotate<FHT>(y2, a.flips + ((size_t)(1 * a.L + l) * 3) * WORDS, gl);
-    const int f1 = group_top_cp<FHT>(y1, gl, a.D, a.log2D, cnt, lv1, lc1);
-    const int f2 = group_top_cp<FHT>(y2, gl, a.D, a.log2D, cnt, lv2, lc2);
-    __syncwarp();
-    bool ok1 = (f1 == cnt), ok2 = (f2 == cnt);
-    for (int t = 1; t < cnt; ++t) {
-      if (ok1 && !(lv1[t - 1] > lv1[t])) ok1 = false;
-      if (ok2 && !(lv2[t - 1] > lv2[t])) ok2 = false;
-    }
-    if (!ok1) {
+#pragma unroll 1
+    for (int layer = 0; layer < 2; ++layer) {
+      float y[E];
 #pragma unroll
-      for (int e = 0; e < E; ++e) ydump[gl * E + e] = y1[e];
-      __syncwarp(gmask);
-      if (gl == 0) replay_layer_topp(ydump, a.D, a.log2D, m1, hv, hi, lv1, lc1);
-      __syncwarp(gmask);
-    }
-    if (!ok2) {
+      for (int e = 0; e < E; ++e) y[e] = xr[e];
+      hd3_rotate<FHT>(y, a.flips + ((size_t)(layer * a.L + l) * 3) * WORDS, gl);
+      float* lv = layer == 0 ? lv1 : lv2;
+      int* lc = layer == 0 ? lc1 : lc2;
+      const int f = group_top_cp_auto<FHT>(y, gl, a.D, a.log2D, cnt, lv, lc);
+      __syncwarp();
+      bool ok = (f == cnt);
+      for (int t = 1; t < cnt; ++t)
+        if (ok && !(lv[t - 1] > lv[t])) ok = false;
+      if (!ok) {
 #pragma unroll
-      for (int e = 0; e < E; ++e) ydump[gl * E + e] = y2[e];
-      __syncwarp(gmask);
-      if (gl == 0) replay_layer_topp(ydump, a.D, a.log2D, m1, hv, hi, lv2, lc2);
-      __syncwarp(gmask);
+        for (int e = 0; e < E; ++e) ydump[gl * E + e] = y[e];
+        __syncwarp(gmask);
+        if (gl == 0) replay_layer_topp(ydump, a.D, a.log2D, m1, hv, hi, lv, lc);
+        __syncwarp(gmask);
+      }
     }
     if (gl == 0 && active) {
       float* ov = a.list_v + ((size_t)q * a.L + l) * m;
@@ -163,7 +157,7 @@ struct SelectArgs {
 __global__ void __launch_bounds__(256) k_probe_select(SelectArgs a, float* hv_g, int* hi_g) {
   __shared__ uint32_t hist[256];
   __shared__ uint32_t s_prefix, s_remaining;
-  __shared__ unsigned s_gt, s_ge, s_out;
+  __shared__ unsigned s_gt, s_ge;
   __shared__ long long tmp[32];
   const int M = a.L * a.m;
   const int Qp = a.qProbes;
@@ -221,7 +215,6 @@ __global__ void __launch_bounds__(256) k_probe_select(SelectArgs a, float* hv_g,
     if (exact) {
       // the selected set is {score >= t}; keep list order (table, rank)
       long long run = 0;
-      if (threadIdx.x == 0) s_out = 0;
       __syncthreads();
       for (int base = 0; base < M; base += blockDim.x) {
         const int i = base + threadIdx.x;

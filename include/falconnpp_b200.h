@@ -100,7 +100,10 @@ int fpp_get_stats(fpp_index* h, int kind, double* out, int n);
 /* Tuning and test switches: "exact_bucket_order" (default 1: bucket contents
  * in the reference's heap order even among equal scores; 0: ascending id among
  * equal scores, the kept set is identical either way), "tables_per_chunk",
- * "stage_timing" (0/1: CUDA events around each query kernel). */
+ * "stage_timing" (0/1: CUDA events around each query kernel), "use_graph"
+ * (0/1: batched form captured into a CUDA graph and replayed for repeated
+ * shapes; the stream must not be the legacy default stream), "blocks_per_sm"
+ * (batched form: resident blocks per SM, 0 = occupancy limit). */
 int fpp_set_option(fpp_index* h, const char* key, long long value);
 
 /* Prints the build report the reference writes to stdout after
@@ -130,6 +133,30 @@ int fpp_build_dump_hash(fpp_index* h, const float* dataset, int32_t* codes, floa
 int fpp_query_dump(fpp_index* h, const float* queries, int n_queries, int n_neighbors, int32_t* out,
                    float* topk_val, uint32_t* probes, float* probe_val, long long* stats, int32_t* cands,
                    long long cand_cap);
+
+/* Selects the implementation behind fpp_query / fpp_query_device (and the
+ * Python query()).  form 0 (default): the plain FP32 path of three kernels,
+ * bit-exact with src/FalconnPP.cpp:310-707.  form 1: the batched path, one
+ * persistent fused kernel per batch (rotate, hash, probe, gather, rerank,
+ * top-k) with dynamic scheduling; precision 0 reranks in FP32 and equals the
+ * plain path bit for bit; precision 1 (BF16) and 2 (FP8-E4M3 with a per-row
+ * scale) rerank the candidates in low precision with FP32 accumulation and
+ * re-score the best shortlist_mult * k of them in exact FP32.  The hashing is
+ * FP32 and identical in every form.  Extends query2Layers_1D; no reference
+ * counterpart for the batched form. */
+int fpp_set_query_form(fpp_index* h, int form, int precision, int shortlist_mult);
+
+/* Batched form with per-query k and qProbes (mixed batches).  d_k and
+ * d_qprobes are device int32 arrays of n_queries entries (NULL: every query
+ * uses k_max / qprobes_max); k_max and qprobes_max bound them.  d_out is
+ * n_queries x out_stride int32 (first k of each row written, descending
+ * score, 0-padded), d_out_val the matching scores or NULL.  Uses the handle's
+ * precision and shortlist setting.  Returns after the results are written.
+ * Limits: qProbes <= 1024, n_tables * ceil(2 qProbes / n_tables) <= 2048,
+ * k * shortlist_mult <= 1024. */
+int fpp_query_batched(fpp_index* h, const float* d_queries, int n_queries, const int32_t* d_k,
+                      const int32_t* d_qprobes, int k_max, int qprobes_max, int32_t* d_out, int out_stride,
+                      float* d_out_val, void* stream);
 
 /* No counterpart in the reference.  The gather, deduplicate, rerank and top-k
  * stage of fpp_query for callers that cannot allocate device memory: code
