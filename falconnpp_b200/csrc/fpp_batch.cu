@@ -195,7 +195,7 @@ constexpr size_t batch_smem_bytes() {
 }
 
 template <int FHT, int MODE, int VI, int VI32>
-__global__ void __launch_bounds__(kBThreads, 2) k_batch_query(BatchArgs a) {
+__global__ void __launch_bounds__(kBThreads, 3) k_batch_query(BatchArgs a) {
   constexpr int E = Geo<FHT>::E;
   constexpr int G = Geo<FHT>::G;
   constexpr int WORDS = Geo<FHT>::WORDS;
@@ -371,40 +371,57 @@ __global__ void __launch_bounds__(kBThreads, 2) k_batch_query(BatchArgs a) {
     __syncthreads();
     const uint32_t C = Qp > 0 ? s_pe[Qp - 1] : 0u;
     const unsigned cap = (unsigned)a.cap;
-    for (uint32_t c0 = (uint32_t)warp * 128u; c0 < C; c0 += kBWarps * 128u) {
-      uint32_t idv[4];
+    {
+      // each warp walks one contiguous slice of the flat candidate range; a
+      // lane finds its probe by stepping forward from the warp's cursor
+      const uint32_t per = (((C + kBWarps - 1) / kBWarps) + 127u) & ~127u;
+      const uint32_t c_begin = min(C, (uint32_t)warp * per);
+      const uint32_t c_end = min(C, c_begin + per);
+      int cur = 0;
+      {
+        int lo = 0, hi = Qp > 0 ? Qp - 1 : 0;
+        while (lo < hi) {
+          const int mid = (lo + hi) >> 1;
+          if (s_pe[mid] > c_begin) hi = mid; else lo = mid + 1;
+        }
+        cur = lo;
+      }
+      for (uint32_t c0 = c_begin; c0 < c_end; c0 += 128u) {
+        uint32_t idv[4];
 #pragma unroll
-      for (int h = 0; h < 4; ++h) {
-        const uint32_t i = c0 + h * 32 + lane;
-        idv[h] = 0xffffffffu;
-        if (i < C) {
-          int lo = 0, hi = Qp - 1;  // first probe whose end exceeds i
-          while (lo < hi) {
-            const int mid = (lo + hi) >> 1;
-            if (s_pe[mid] > i) hi = mid; else lo = mid + 1;
+        for (int h = 0; h < 4; ++h) {
+          const uint32_t i = c0 + h * 32 + lane;
+          idv[h] = 0xffffffffu;
+          if (i < c_end) {
+            int p = cur;
+            while (s_pe[p] <= i) ++p;
+            const uint32_t st = p > 0 ? s_pe[p - 1] : 0u;
+            idv[h] = (uint32_t)__ldg(a.ids + s_po[p] + (i - st));
           }
-          const uint32_t st = lo > 0 ? s_pe[lo - 1] : 0u;
-          idv[h] = (uint32_t)__ldg(a.ids + s_po[lo] + (i - st));
         }
-      }
-      bool fresh[4];
-#pragma unroll
-      for (int h = 0; h < 4; ++h) {
-        fresh[h] = false;
-        if (idv[h] != 0xffffffffu) {
-          const uint32_t bit = 1u << (idv[h] & 31u);
-          fresh[h] = (atomicOr(bits + (idv[h] >> 5), bit) & bit) == 0u;
+        {  // advance the cursor to the probe holding the next step's first id
+          const uint32_t nxt = min(c0 + 128u, c_end > 0 ? c_end - 1 : 0u);
+          while (cur < Qp - 1 && s_pe[cur] <= nxt) ++cur;
         }
-      }
+        bool fresh[4];
 #pragma unroll
-      for (int h = 0; h < 4; ++h) {
-        const unsigned bal = __ballot_sync(kFullMask, fresh[h]);
-        if (bal) {
-          unsigned base = 0;
-          if (lane == 0) base = atomicAdd(&s_u, (unsigned)__popc(bal));
-          base = __shfl_sync(kFullMask, base, 0);
-          const unsigned pos = base + __popc(bal & ((1u << lane) - 1u));
-          if (fresh[h] && pos < cap) uq[pos] = idv[h];
+        for (int h = 0; h < 4; ++h) {
+          fresh[h] = false;
+          if (idv[h] != 0xffffffffu) {
+            const uint32_t bit = 1u << (idv[h] & 31u);
+            fresh[h] = (atomicOr(bits + (idv[h] >> 5), bit) & bit) == 0u;
+          }
+        }
+#pragma unroll
+        for (int h = 0; h < 4; ++h) {
+          const unsigned bal = __ballot_sync(kFullMask, fresh[h]);
+          if (bal) {
+            unsigned base = 0;
+            if (lane == 0) base = atomicAdd(&s_u, (unsigned)__popc(bal));
+            base = __shfl_sync(kFullMask, base, 0);
+            const unsigned pos = base + __popc(bal & ((1u << lane) - 1u));
+            if (fresh[h] && pos < cap) uq[pos] = idv[h];
+          }
         }
       }
     }

@@ -230,12 +230,69 @@ __device__ __forceinline__ int group_top_cp_small(const float (&y)[Geo<FHT>::E],
   return found;
 }
 
+// cnt <= 2 (the query path with one probe per layer, the build with
+// iProbes = 1): lane-local top-2 on |y| with compile-time element indices,
+// then at most two merge rounds.  |y| compares exactly like sgn(y)*y
+// (-0 and +0 are equal); the reported value keeps the reference's sign rule.
+template <int FHT>
+__device__ __forceinline__ int group_top2_cp(const float (&y)[Geo<FHT>::E], int gl, int D, int log2D, int cnt,
+                                             float* out_v, int* out_c) {
+  constexpr int E = Geo<FHT>::E;
+  constexpr int G = Geo<FHT>::G;
+  const int lim = D - gl * E;  // elements of this lane that are coordinates (< D)
+  float b0 = -1.0f, b1 = -1.0f, s0 = 0.0f, s1 = 0.0f;
+  int e0 = E, e1 = E;
+#pragma unroll
+  for (int e = 0; e < E; ++e) {
+    const float v = fabsf(y[e]);
+    const bool ok = e < lim;
+    const bool g0 = ok && v > b0;
+    const bool g1 = ok && v > b1;
+    b1 = g0 ? b0 : (g1 ? v : b1);
+    s1 = g0 ? s0 : (g1 ? y[e] : s1);
+    e1 = g0 ? e0 : (g1 ? e : e1);
+    b0 = g0 ? v : b0;
+    s0 = g0 ? y[e] : s0;
+    e0 = g0 ? e : e0;
+  }
+  int found = 0;
+  bool took0 = false;
+  for (int t = 0; t < cnt; ++t) {
+    const float hv = took0 ? b1 : b0;
+    const int he = took0 ? e1 : e0;
+    float wv = hv;
+    int wr = he < E ? gl * E + he : 0x7fffffff;
+    const int myr = wr;
+#pragma unroll
+    for (int s = 1; s < G; s <<= 1) {
+      const float ov = __shfl_xor_sync(kFullMask, wv, s);
+      const int orr = __shfl_xor_sync(kFullMask, wr, s);
+      if (cp_better(ov, orr, wv, wr)) {
+        wv = ov;
+        wr = orr;
+      }
+    }
+    if (wr == 0x7fffffff) break;
+    const bool mine = (wr == myr);
+    const float sy = took0 ? s1 : s0;
+    const int owner = (threadIdx.x & 31 & ~(G - 1)) + wr / E;
+    const float wy = __shfl_sync(kFullMask, sy, owner);
+    if (mine) took0 = true;
+    if (gl == 0) {
+      out_v[t] = cp_value(wy);
+      out_c[t] = cp_code(wy, wr, log2D);
+    }
+    ++found;
+  }
+  return found;
+}
+
 // Dispatch: the single-pass selection when cnt is small, the round-based one
 // otherwise.
 template <int FHT>
 __device__ __forceinline__ int group_top_cp_auto(const float (&y)[Geo<FHT>::E], int gl, int D, int log2D, int cnt,
                                                  float* out_v, int* out_c) {
-  if (cnt <= 2) return group_top_cp_small<FHT, 2>(y, gl, D, log2D, cnt, out_v, out_c);
+  if (cnt <= 2) return group_top2_cp<FHT>(y, gl, D, log2D, cnt, out_v, out_c);
   if (cnt <= 4) return group_top_cp_small<FHT, 4>(y, gl, D, log2D, cnt, out_v, out_c);
   return group_top_cp<FHT>(y, gl, D, log2D, cnt, out_v, out_c);
 }
