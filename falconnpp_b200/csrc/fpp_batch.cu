@@ -31,10 +31,14 @@ namespace fpp {
 
 constexpr int kBThreads = 256;
 constexpr int kBWarps = kBThreads / 32;
-constexpr int kBMaxList = 2048;   // L * m entries held in shared memory
+constexpr int kBMaxList = 1024;   // L * m entries held in shared memory
 constexpr int kBMaxProbes = 1024;
 constexpr int kBMaxM1 = 16;
 constexpr int kBMaxTop = 1024;    // k * shortlist multiple, and the replay heaps
+constexpr int kHT = 8192;         // shared-memory hash set for the dedupe (2^13 slots)
+constexpr unsigned kHTLimit = kHT - 2048;  // unique ids before switching to the L2 bitset
+constexpr uint32_t kEmpty = 0xffffffffu;
+constexpr int kHistBins = 2048;   // top 11 bits of the score key
 
 struct BatchArgs {
   const float* Xc;
@@ -149,39 +153,48 @@ __device__ __forceinline__ void block_sort_u64(unsigned long long* a, int n) {
     }
 }
 
-// dynamic shared memory of k_batch_query
+// dynamic shared memory of k_batch_query (regions reused phase by phase)
 template <int GROUPS>
 struct BatchSmem {
-  static constexpr size_t kLv = 0;
+  static constexpr size_t kHt = 0;                              // hash set (gather)
+  static constexpr size_t kLv = kHt + 4 * kHT;                  // lists (hash, select)
   static constexpr size_t kLb = kLv + 4 * kBMaxList;
   static constexpr size_t kProbe = kLb + 4 * kBMaxList;
-  static constexpr size_t kTop = kProbe + 4 * kBMaxProbes;
-  static constexpr size_t kHv = kTop + 8 * kBMaxTop;
-  static constexpr size_t kHi = kHv + 4 * kBMaxTop;
-  static constexpr size_t kGv = kHi + 4 * kBMaxTop;
+  static constexpr size_t kTop = kProbe + 4 * kBMaxProbes;      // sorted (key, id) of the top-k stage
+  static constexpr size_t kGv = kTop + 8 * kBMaxTop;
   static constexpr size_t kGc = kGv + 4 * GROUPS * 2 * (kBMaxM1 + 1);
   static constexpr size_t kRhv = kGc + 4 * GROUPS * 2 * (kBMaxM1 + 1);
   static constexpr size_t kRhi = kRhv + 4 * GROUPS * kBMaxM1;
   static constexpr size_t kQ = kRhi + 4 * GROUPS * kBMaxM1;
   static constexpr size_t kBytes = kQ + 4 * 1024;
+  uint32_t* ht;
   float* lv;
   uint32_t* lb;
   uint32_t* probe;
   unsigned long long* top;
-  float* hv;
-  int* hi;
   float* gv;
   int* gc;
   float* rhv;
   int* rhi;
   float* q;  // the current query, zero padded to 1024 floats
+  // aliases: gather prefix arrays over the lists; the score histogram over
+  // both lists (2048 u32); the probe-cut replay heap in the top region; the
+  // re-score arrays and the final replay heap in the hash-set region
+  __device__ uint32_t* po() const { return lb; }
+  __device__ uint32_t* pe() const { return reinterpret_cast<uint32_t*>(lv); }
+  __device__ uint32_t* hist() const { return reinterpret_cast<uint32_t*>(lv); }
+  __device__ float* phv() const { return reinterpret_cast<float*>(top); }
+  __device__ int* phi() const { return reinterpret_cast<int*>(top) + 512; }
+  __device__ uint32_t* sid() const { return ht; }
+  __device__ uint32_t* ssc() const { return ht + 1024; }
+  __device__ float* fhv() const { return reinterpret_cast<float*>(ht + 2048); }
+  __device__ int* fhi() const { return reinterpret_cast<int*>(ht + 3072); }
   __device__ explicit BatchSmem(unsigned char* p)
-      : lv(reinterpret_cast<float*>(p + kLv)),
+      : ht(reinterpret_cast<uint32_t*>(p + kHt)),
+        lv(reinterpret_cast<float*>(p + kLv)),
         lb(reinterpret_cast<uint32_t*>(p + kLb)),
         probe(reinterpret_cast<uint32_t*>(p + kProbe)),
         top(reinterpret_cast<unsigned long long*>(p + kTop)),
-        hv(reinterpret_cast<float*>(p + kHv)),
-        hi(reinterpret_cast<int*>(p + kHi)),
         gv(reinterpret_cast<float*>(p + kGv)),
         gc(reinterpret_cast<int*>(p + kGc)),
         rhv(reinterpret_cast<float*>(p + kRhv)),
@@ -193,6 +206,8 @@ template <int FHT>
 constexpr size_t batch_smem_bytes() {
   return BatchSmem<kBThreads / Geo<FHT>::G>::kBytes;
 }
+
+__device__ __forceinline__ uint32_t ht_slot(uint32_t id) { return (id * 2654435761u) >> (32 - 13); }
 
 template <int FHT, int MODE, int VI, int VI32>
 __global__ void __launch_bounds__(kBThreads, 3) k_batch_query(BatchArgs a) {
@@ -206,11 +221,9 @@ __global__ void __launch_bounds__(kBThreads, 3) k_batch_query(BatchArgs a) {
   uint32_t* s_lb = sm.lb;
   uint32_t* s_probe = sm.probe;
   unsigned long long* s_top = sm.top;
-  float* s_hv = sm.hv;
-  int* s_hi = sm.hi;
   __shared__ uint32_t hist[256];
   __shared__ uint32_t s_pre, s_rem;
-  __shared__ unsigned s_cnt, s_u, s_sel, s_q;
+  __shared__ unsigned s_cnt, s_u, s_sel, s_q, s_ovf, s_bstar, s_above;
   __shared__ long long tmp[32];
 
   const int tid = threadIdx.x;
@@ -227,8 +240,10 @@ __global__ void __launch_bounds__(kBThreads, 3) k_batch_query(BatchArgs a) {
   float* ph_v = a.gheap_v + gid * (long long)a.mmax;
   int* ph_i = a.gheap_i + gid * (long long)a.mmax;
   const int L = a.L;
+  for (int i = tid; i < kHT; i += kBThreads) sm.ht[i] = kEmpty;
 
   for (;;) {
+    __syncthreads();
     if (tid == 0) s_q = atomicAdd(a.work, 1u);
     __syncthreads();
     const unsigned qu = s_q;
@@ -239,7 +254,6 @@ __global__ void __launch_bounds__(kBThreads, 3) k_batch_query(BatchArgs a) {
     if (k < 1 || k > a.k_max || Qp < 1 || Qp > a.qprobes_max) {  // block-uniform
       if (tid == 0) atomicOr(a.status, 2u);
       for (int j = tid; j < a.out_stride; j += kBThreads) a.out[(size_t)q * a.out_stride + j] = -1;
-      __syncthreads();
       continue;
     }
     const int m = (2 * Qp + L - 1) / L;  // ceil(2.0 * qProbes / L), FalconnPP.cpp:336
@@ -310,45 +324,56 @@ __global__ void __launch_bounds__(kBThreads, 3) k_batch_query(BatchArgs a) {
     }
     __syncthreads();
 
-    // ---- 2. global top-qProbes of the L*m lists (FalconnPP.cpp:540-582)
+    // ---- 2. global top-qProbes of the L*m lists (FalconnPP.cpp:540-582):
+    // rank by counting; a tie straddling the cut replays the reference's heap
     {
-      unsigned ge;
-      const uint32_t t = block_select(M, (unsigned)Qp, [&](int i) { return ord_key(s_lv[i]); }, hist, &s_pre,
-                                      &s_rem, &s_cnt, &ge);
-      if (ge == (unsigned)Qp) {
-        long long run = 0;
-        for (int base = 0; base < M; base += kBThreads) {
-          const int i = base + tid;
-          const bool take = i < M && ord_key(s_lv[i]) >= t;
-          long long tot;
-          const long long pos = block_exclusive_scan(take ? 1 : 0, tmp, &tot) + run;
-          if (take) s_probe[pos] = s_lb[i];
-          run += tot;
+      long long run = 0;
+      bool tie = false;
+      for (int base = 0; base < M; base += kBThreads) {
+        const int i = base + tid;
+        bool take = false;
+        if (i < M) {
+          const uint32_t ki = ord_key(s_lv[i]);
+          int gt = 0, eq = 0;
+          for (int j = 0; j < M; ++j) {
+            const uint32_t kj = ord_key(s_lv[j]);
+            gt += kj > ki;
+            eq += kj == ki;
+          }
+          take = gt < Qp;
+          tie |= take && gt + eq > Qp;
         }
-      } else if (tid == 0) {
+        long long tot;
+        const long long pos = block_exclusive_scan(take ? 1 : 0, tmp, &tot) + run;
+        if (take && pos < Qp) s_probe[pos] = s_lb[i];
+        run += tot;
+      }
+      if (__syncthreads_or(tie) && tid == 0) {
+        float* hv = sm.phv();
+        int* hi = sm.phi();
+        int* track = hi + L;
         int n = 0;
-        int* track = s_hi + L;
         for (int l = 0; l < L; ++l) {
-          heap_push<false, int>(s_hv, s_hi, n, s_lv[l * m], l * m);
+          heap_push<false, int>(hv, hi, n, s_lv[l * m], l * m);
           track[l] = 0;
         }
         for (int pc = 0; pc < Qp; ++pc) {
-          const int pos = s_hi[0];
-          heap_pop<false, int>(s_hv, s_hi, n);
+          const int pos = hi[0];
+          heap_pop<false, int>(hv, hi, n);
           s_probe[pc] = s_lb[pos];
           const int tb = pos / m;
           track[tb]++;
-          if (track[tb] < m) heap_push<false, int>(s_hv, s_hi, n, s_lv[tb * m + track[tb]], tb * m + track[tb]);
+          if (track[tb] < m) heap_push<false, int>(hv, hi, n, s_lv[tb * m + track[tb]], tb * m + track[tb]);
         }
       }
       __syncthreads();
     }
 
-    // ---- 3. gather + dedupe (FalconnPP.cpp:584-606), the candidates of all
-    // probes flattened over the block's warps, 128 ids per warp step
-    if (tid == 0) s_u = 0;
-    uint32_t* s_po = s_lb;                                // bucket start of probe p
-    uint32_t* s_pe = reinterpret_cast<uint32_t*>(s_lv);  // inclusive end of probe p in the flat range
+    // ---- 3. gather + dedupe (FalconnPP.cpp:584-606): the candidates of all
+    // probes flattened over the warps; dedupe in a shared-memory hash set, or
+    // (when a query has too many unique ids) in the block's L2 bitset
+    uint32_t* s_po = sm.po();
+    uint32_t* s_pe = sm.pe();
     {
       long long run = 0;
       for (int base = 0; base < Qp; base += kBThreads) {
@@ -368,18 +393,21 @@ __global__ void __launch_bounds__(kBThreads, 3) k_batch_query(BatchArgs a) {
         run += tot;
       }
     }
+    if (tid == 0) {
+      s_u = 0;
+      s_ovf = 0;
+    }
     __syncthreads();
-    const uint32_t C = Qp > 0 ? s_pe[Qp - 1] : 0u;
+    const uint32_t C = s_pe[Qp - 1];
     const unsigned cap = (unsigned)a.cap;
-    {
-      // each warp walks one contiguous slice of the flat candidate range; a
-      // lane finds its probe by stepping forward from the warp's cursor
+    bool use_bitset = false;
+    for (int pass = 0; pass < 2; ++pass) {
       const uint32_t per = (((C + kBWarps - 1) / kBWarps) + 127u) & ~127u;
       const uint32_t c_begin = min(C, (uint32_t)warp * per);
       const uint32_t c_end = min(C, c_begin + per);
       int cur = 0;
       {
-        int lo = 0, hi = Qp > 0 ? Qp - 1 : 0;
+        int lo = 0, hi = Qp - 1;
         while (lo < hi) {
           const int mid = (lo + hi) >> 1;
           if (s_pe[mid] > c_begin) hi = mid; else lo = mid + 1;
@@ -387,11 +415,12 @@ __global__ void __launch_bounds__(kBThreads, 3) k_batch_query(BatchArgs a) {
         cur = lo;
       }
       for (uint32_t c0 = c_begin; c0 < c_end; c0 += 128u) {
+        if (!use_bitset && *(volatile unsigned*)&s_ovf) break;
         uint32_t idv[4];
 #pragma unroll
         for (int h = 0; h < 4; ++h) {
           const uint32_t i = c0 + h * 32 + lane;
-          idv[h] = 0xffffffffu;
+          idv[h] = kEmpty;
           if (i < c_end) {
             int p = cur;
             while (s_pe[p] <= i) ++p;
@@ -399,17 +428,33 @@ __global__ void __launch_bounds__(kBThreads, 3) k_batch_query(BatchArgs a) {
             idv[h] = (uint32_t)__ldg(a.ids + s_po[p] + (i - st));
           }
         }
-        {  // advance the cursor to the probe holding the next step's first id
-          const uint32_t nxt = min(c0 + 128u, c_end > 0 ? c_end - 1 : 0u);
+        {
+          const uint32_t nxt = min(c0 + 128u, c_end - 1);
           while (cur < Qp - 1 && s_pe[cur] <= nxt) ++cur;
         }
         bool fresh[4];
 #pragma unroll
         for (int h = 0; h < 4; ++h) {
           fresh[h] = false;
-          if (idv[h] != 0xffffffffu) {
-            const uint32_t bit = 1u << (idv[h] & 31u);
-            fresh[h] = (atomicOr(bits + (idv[h] >> 5), bit) & bit) == 0u;
+          const uint32_t id = idv[h];
+          if (id != kEmpty) {
+            if (use_bitset) {
+              const uint32_t bit = 1u << (id & 31u);
+              fresh[h] = (atomicOr(bits + (id >> 5), bit) & bit) == 0u;
+            } else {
+              // linear probing; the table never holds more than kHTLimit +
+              // 1024 ids, so an empty slot always exists
+              uint32_t slot = ht_slot(id);
+              for (;;) {
+                const uint32_t old = atomicCAS(sm.ht + slot, kEmpty, id);
+                if (old == kEmpty) {
+                  fresh[h] = true;
+                  break;
+                }
+                if (old == id) break;
+                slot = (slot + 1) & (kHT - 1);
+              }
+            }
           }
         }
 #pragma unroll
@@ -423,9 +468,16 @@ __global__ void __launch_bounds__(kBThreads, 3) k_batch_query(BatchArgs a) {
             if (fresh[h] && pos < cap) uq[pos] = idv[h];
           }
         }
+        if (!use_bitset && lane == 0 && *(volatile unsigned*)&s_u >= kHTLimit) s_ovf = 1u;
       }
+      __syncthreads();
+      if (use_bitset || !s_ovf) break;
+      // too many unique ids for the hash set: start over with the bitset
+      for (int i = tid; i < kHT; i += kBThreads) sm.ht[i] = kEmpty;
+      if (tid == 0) s_u = 0;
+      use_bitset = true;
+      __syncthreads();
     }
-    __syncthreads();
     const unsigned U = s_u;
     int32_t* orow = a.out + (size_t)q * a.out_stride;
     float* ovrow = a.out_v ? a.out_v + (size_t)q * a.out_stride : nullptr;
@@ -436,15 +488,19 @@ __global__ void __launch_bounds__(kBThreads, 3) k_batch_query(BatchArgs a) {
         if (ovrow) ovrow[j] = 0.0f;
       }
       for (long long w = tid; w < a.nwords; w += kBThreads) bits[w] = 0u;
-      __syncthreads();
+      for (int i = tid; i < kHT; i += kBThreads) sm.ht[i] = kEmpty;
       continue;
     }
 
-    // ---- 4. rerank the unique rows (FalconnPP.cpp:642-660)
+    // ---- 4. rerank the unique rows (FalconnPP.cpp:642-660), with a
+    // histogram of the scores' top 11 key bits for the selection below
+    uint32_t* s_hist = sm.hist();
+    for (int i = tid; i < kHistBins; i += kBThreads) s_hist[i] = 0u;
+    __syncthreads();
     {
       const float* scl = MODE == kRowsFP8 ? a.Xscale : nullptr;
       rerank_rows<MODE, VI, (MODE == kRowsF32 ? 2 : 4)>(uq, U, sc, sm.q, a.Xrows, a.row_bytes, a.nchunk, scl,
-                                                           warp, kBWarps, lane);
+                                                           warp, kBWarps, lane, s_hist);
     }
     __syncthreads();
 
@@ -454,48 +510,88 @@ __global__ void __launch_bounds__(kBThreads, 3) k_batch_query(BatchArgs a) {
     unsigned nsel = U;
     bool exact = true;
     if (U > R) {
-      unsigned ge;
-      const uint32_t t = block_select((int)U, R, [&](int i) { return ord_key_bits(sc[i]); }, hist, &s_pre, &s_rem,
-                                      &s_cnt, &ge);
-      if (MODE == kRowsF32 && ge != R) {
-        exact = false;  // tie at the k-th score: replay below
-      } else {
-        // keep every entry >= t (ties at the cut included, at most kBMaxTop)
+      // the bin holding the R-th largest key: thread t owns bins
+      // [2048 - 8(t+1), 2048 - 8t), scanned from the top
+      {
+        uint32_t c[8];
+        uint32_t sum = 0;
+        const int hi = kHistBins - 8 * tid;
+#pragma unroll
+        for (int b = 0; b < 8; ++b) {
+          c[b] = s_hist[hi - 1 - b];
+          sum += c[b];
+        }
+        long long tot;
+        const long long above = block_exclusive_scan((long long)sum, tmp, &tot);
+        if (above < (long long)R && above + sum >= R) {
+          long long cum = above;
+#pragma unroll
+          for (int b = 0; b < 8; ++b) {
+            if (cum + c[b] >= R && cum < (long long)R) {
+              s_bstar = (uint32_t)(hi - 1 - b);
+              s_above = (uint32_t)(cum + c[b]);
+            }
+            cum += c[b];
+          }
+        }
+      }
+      __syncthreads();
+      const uint32_t bstar = s_bstar;
+      if (s_above <= (unsigned)kBMaxTop) {
         if (tid == 0) s_sel = 0;
         __syncthreads();
         for (unsigned i = tid; i < U; i += kBThreads) {
           const uint32_t key = ord_key_bits(sc[i]);
-          if (key >= t) {
+          if ((key >> 21) >= bstar) {
             const unsigned pos = atomicAdd(&s_sel, 1u);
-            if (pos < (unsigned)kBMaxTop) s_top[pos] = ((unsigned long long)(~key) << 32) | uq[i];
+            s_top[pos] = ((unsigned long long)(~key) << 32) | uq[i];
           }
         }
         __syncthreads();
-        nsel = min(s_sel, (unsigned)kBMaxTop);
+        nsel = s_sel;
+      } else {
+        // very many equal top bits: radix selection of the R-th key
+        unsigned ge;
+        const uint32_t t = block_select((int)U, R, [&](int i) { return ord_key_bits(sc[i]); }, hist, &s_pre,
+                                        &s_rem, &s_cnt, &ge);
+        if (MODE == kRowsF32 && ge != R) {
+          exact = false;
+        } else {
+          if (tid == 0) s_sel = 0;
+          __syncthreads();
+          for (unsigned i = tid; i < U; i += kBThreads) {
+            const uint32_t key = ord_key_bits(sc[i]);
+            if (key >= t) {
+              const unsigned pos = atomicAdd(&s_sel, 1u);
+              if (pos < (unsigned)kBMaxTop) s_top[pos] = ((unsigned long long)(~key) << 32) | uq[i];
+            }
+          }
+          __syncthreads();
+          nsel = min(s_sel, (unsigned)kBMaxTop);
+        }
       }
     } else {
       for (unsigned i = tid; i < U; i += kBThreads)
         s_top[i] = ((unsigned long long)(~ord_key_bits(sc[i])) << 32) | uq[i];
       __syncthreads();
     }
-    if (exact && MODE != kRowsF32) {
-      // exact FP32 re-score of the shortlist with the parity dot order
-      __syncthreads();
-      if (nsel > 0) {
-        uint32_t* sid = reinterpret_cast<uint32_t*>(s_hv);  // shortlist ids
-        uint32_t* ssc = reinterpret_cast<uint32_t*>(s_hi);  // their FP32 scores
+    if (exact) {
+      block_sort_u64(s_top, (int)nsel);
+      if (MODE != kRowsF32) {
+        // exact FP32 re-score of the best R with the parity dot order
+        nsel = min(nsel, R);
+        uint32_t* sid = sm.sid();
+        uint32_t* ssc = sm.ssc();
         for (unsigned i = tid; i < nsel; i += kBThreads) sid[i] = (uint32_t)s_top[i];
         __syncthreads();
         rerank_rows<kRowsF32, VI32>(sid, nsel, ssc, sm.q, reinterpret_cast<const unsigned char*>(a.Xc),
-                                    (size_t)a.ld * 4, a.ld / 4, nullptr, warp, kBWarps, lane);
+                                    (size_t)a.ld * 4, a.ld / 4, nullptr, warp, kBWarps, lane, nullptr);
         __syncthreads();
         for (unsigned i = tid; i < nsel; i += kBThreads)
           s_top[i] = ((unsigned long long)(~ord_key_bits(ssc[i])) << 32) | sid[i];
         __syncthreads();
+        block_sort_u64(s_top, (int)nsel);
       }
-    }
-    if (exact) {
-      block_sort_u64(s_top, (int)nsel);
       const unsigned kept = min(nsel, kk);
       unsigned dup = 0;
       // equal FP32 scores in the kept list, or at the k-th place: heap order decides
@@ -513,11 +609,12 @@ __global__ void __launch_bounds__(kBThreads, 3) k_batch_query(BatchArgs a) {
         }
       }
     }
+    bool bits_dirty = use_bitset;
     if (!exact) {
       // the reference's min-heap over the candidates in ascending id order
       // (FalconnPP.cpp:633-673): all of them in FP32 mode, the shortlist otherwise
       const bool whole = (MODE == kRowsF32);
-      unsigned nc = whole ? U : nsel;
+      const unsigned nc = whole ? U : nsel;
       uint32_t* cid = uq;
       uint32_t* csc = sc;
       if (!whole) {
@@ -526,31 +623,33 @@ __global__ void __launch_bounds__(kBThreads, 3) k_batch_query(BatchArgs a) {
           csc[i] = ord_key_inv_dev(~(uint32_t)(s_top[i] >> 32));
         }
         __syncthreads();
+        if (use_bitset) {  // the unique list was overwritten: clear every word
+          for (long long w = tid; w < a.nwords; w += kBThreads) bits[w] = 0u;
+          bits_dirty = false;
+        }
       }
       block_bitonic_sort_u32(cid, csc, (int)nc);
       if (tid == 0) {
+        float* hv = sm.fhv();
+        int* hi = sm.fhi();
         int n = 0;
-        for (unsigned i = 0; i < nc; ++i) topp_offer<int>(s_hv, s_hi, n, k, __uint_as_float(csc[i]), (int)cid[i]);
+        for (unsigned i = 0; i < nc; ++i) topp_offer<int>(hv, hi, n, k, __uint_as_float(csc[i]), (int)cid[i]);
         for (int j = n; j < k; ++j) {
           orow[j] = 0;
           if (ovrow) ovrow[j] = 0.0f;
         }
         for (int j = n - 1; j >= 0; --j) {
-          orow[j] = s_hi[0];
-          if (ovrow) ovrow[j] = s_hv[0];
-          heap_pop<true, int>(s_hv, s_hi, n);
+          orow[j] = hi[0];
+          if (ovrow) ovrow[j] = hv[0];
+          heap_pop<true, int>(hv, hi, n);
         }
       }
       __syncthreads();
-      if (!whole) {  // the unique list was overwritten: clear the whole bitset
-        for (long long w = tid; w < a.nwords; w += kBThreads) bits[w] = 0u;
-        __syncthreads();
-        continue;
-      }
     }
-    __syncthreads();
-    for (unsigned i = tid; i < U; i += kBThreads) bits[uq[i] >> 5] = 0u;
-    __syncthreads();
+    // ---- 6. leave the hash set empty and the bitset clear
+    for (int i = tid; i < kHT; i += kBThreads) sm.ht[i] = kEmpty;
+    if (bits_dirty)
+      for (unsigned i = tid; i < U; i += kBThreads) bits[uq[i] >> 5] = 0u;
   }
 }
 
@@ -712,11 +811,10 @@ int batch_query(const Params& P, DeviceIndex& di, BatchWorkspace& bw, const Batc
   const int mmax = (2 * rq.qprobes_max + L - 1) / L;
   int m1max = 0;
   while (m1max * m1max < mmax) ++m1max;
-  if (rq.qprobes_max > kBMaxProbes || (long long)L * mmax > kBMaxList || m1max > kBMaxM1 || m1max > D ||
-      L > kBMaxTop / 2) {
+  if (rq.qprobes_max > kBMaxProbes || (long long)L * mmax > kBMaxList || m1max > kBMaxM1 || m1max > D || L > 512) {
     err.code = kErrUnsupported;
-    err.msg = "batch query: qProbes too large for the batched form (at most 2048 probes, n_tables * probes per "
-              "table <= 4096, ceil(sqrt(probes per table)) <= 16); use the plain form";
+    err.msg = "batch query: outside the batched form's limits (qProbes <= 1024, n_tables * probes per table <= "
+              "1024, ceil(sqrt(probes per table)) <= 16, n_tables <= 512); use the plain form";
     return err.code;
   }
   if (rq.k_max < 1 || (long long)rq.k_max * (rq.mode == kRowsF32 ? 1 : rq.shortlist_mult) > kBMaxTop) {

@@ -16,6 +16,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "fpp_heap.h"
+
 namespace fpp {
 
 enum RowMode : int { kRowsF32 = 0, kRowsBF16 = 1, kRowsFP8 = 2 };
@@ -71,11 +73,13 @@ __device__ __forceinline__ void unpack_chunk(const uint4& u, float* x) {
 // STEPS steps at a time (all their loads in flight together).  qs is the query in shared memory, zero-padded to
 // nchunk * elements-per-chunk floats; row_bytes is the row stride in bytes
 // (multiple of 16); nchunk the 16-byte chunks that hold the d elements; scale
-// (FP8 only) the per-row factor.
+// (FP8 only) the per-row factor; hist11, when given, counts the scores by the
+// top 11 bits of their order-preserving key.
 template <int MODE, int VI, int STEPS = 2>
 __device__ __forceinline__ void rerank_rows(const uint32_t* ids, unsigned U, uint32_t* score, const float* qs,
                                             const unsigned char* rows, size_t row_bytes, int nchunk,
-                                            const float* scale, int warp, int nwarps, int lane) {
+                                            const float* scale, int warp, int nwarps, int lane,
+                                            uint32_t* hist11 = nullptr) {
   constexpr int EPC = RowFmt<MODE>::EPC;
   const int j = lane & 7;
   const int rsub = lane >> 3;  // which of the warp's 4 rows
@@ -127,7 +131,10 @@ __device__ __forceinline__ void rerank_rows(const uint32_t* ids, unsigned U, uin
       t = __fadd_rn(t, __shfl_xor_sync(0xffffffffu, t, 2));
       t = __fadd_rn(t, __shfl_xor_sync(0xffffffffu, t, 1));
       if (MODE == kRowsFP8) t = __fmul_rn(t, live[s] ? __ldg(scale + rid[s]) : 0.0f);
-      if (j == 0 && live[s]) score[base + s * 4 + rsub] = __float_as_uint(t);
+      if (j == 0 && live[s]) {
+        score[base + s * 4 + rsub] = __float_as_uint(t);
+        if (hist11) atomicAdd(hist11 + (ord_key_bits(__float_as_uint(t)) >> 21), 1u);
+      }
     }
   }
 }
