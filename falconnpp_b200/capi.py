@@ -19,7 +19,8 @@ EXPORTED = [
     "fpp_build", "fpp_build_device", "fpp_query", "fpp_query_device", "fpp_last_error", "fpp_get_info",
     "fpp_get_stats", "fpp_set_option", "fpp_print_build_report", "fpp_dump_bits", "fpp_dump_center",
     "fpp_dump_tables", "fpp_build_dump_hash", "fpp_query_dump", "fpp_rerank_probes_noalloc",
-    "fpp_set_query_form", "fpp_query_batched",
+    "fpp_set_query_form", "fpp_query_batched", "fpp_autotune",
+    "fpp_server_create", "fpp_server_submit", "fpp_server_wait", "fpp_server_stats", "fpp_server_destroy",
 ]
 
 _lib = None
@@ -62,6 +63,12 @@ def lib() -> ctypes.CDLL:
             "fpp_rerank_probes_noalloc": (i32, [vp, vp, i32, vp, i32, i32, vp, vp]),
             "fpp_set_query_form": (i32, [vp, i32, i32, i32]),
             "fpp_query_batched": (i32, [vp, vp, i32, vp, vp, i32, i32, vp, i32, vp, vp]),
+            "fpp_autotune": (i32, [vp, vp, i32, i32, ctypes.c_double, vp, vp]),
+            "fpp_server_create": (i32, [vp, i32, i64, i32, i32, i32, ctypes.POINTER(vp)]),
+            "fpp_server_submit": (i32, [vp, vp, i32, i32, i32, vp, ctypes.POINTER(i64)]),
+            "fpp_server_wait": (i32, [vp, i64, ctypes.POINTER(ctypes.c_double)]),
+            "fpp_server_stats": (i32, [vp, vp, i32]),
+            "fpp_server_destroy": (None, [vp]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -159,6 +166,13 @@ class Index:
                                        ctypes.c_void_p(qp_ptr or 0), k_max, qp_max, ctypes.c_void_p(out_ptr),
                                        out_stride, ctypes.c_void_p(val_ptr or 0), ctypes.c_void_p(stream or 0)))
 
+    def autotune(self, q_ptr: int, nq: int, k: int, min_agreement: float = 0.99, stream: int | None = None) -> dict:
+        rep = np.zeros(6, np.float64)
+        _check(lib().fpp_autotune(self.h, ctypes.c_void_p(q_ptr), nq, k, min_agreement, _ptr(rep),
+                                  ctypes.c_void_p(stream or 0)))
+        return dict(ms=rep[0], blocks_per_sm=int(rep[1]), precision=int(rep[2]), shortlist_mult=int(rep[3]),
+                    agreement=rep[4], tried=int(rep[5]))
+
     def info(self) -> dict:
         v = np.zeros(6, np.int64)
         _check(lib().fpp_get_info(self.h, _ptr(v), 6))
@@ -189,3 +203,46 @@ class Index:
         ids = np.zeros(max(1, info["n_ids"]), np.int32)
         _check(lib().fpp_dump_tables(self.h, _ptr(start), _ptr(ids)))
         return start, ids[: info["n_ids"]]
+
+
+class Server:
+    """Continuous-batching serving loop over an Index (fpp_server_*)."""
+
+    def __init__(self, index: Index, n_streams=3, memory_budget=1 << 30, max_batch=8192, k_max=100,
+                 qprobes_max=80):
+        self.index = index
+        h = ctypes.c_void_p()
+        _check(lib().fpp_server_create(index.h, n_streams, memory_budget, max_batch, k_max, qprobes_max,
+                                       ctypes.byref(h)))
+        self.h = h
+        self._keep = {}
+
+    def submit(self, Q: np.ndarray, k: int, qprobes: int) -> int:
+        Q = np.ascontiguousarray(Q, np.float32)
+        out = np.zeros((Q.shape[0], k), np.int32)
+        t = ctypes.c_longlong()
+        _check(lib().fpp_server_submit(self.h, _ptr(Q), Q.shape[0], k, qprobes, _ptr(out), ctypes.byref(t)))
+        self._keep[t.value] = (Q, out)
+        return t.value
+
+    def wait(self, ticket: int):
+        lat = ctypes.c_double()
+        _check(lib().fpp_server_wait(self.h, ticket, ctypes.byref(lat)))
+        _, out = self._keep.pop(ticket)
+        return out, lat.value
+
+    def stats(self) -> dict:
+        v = np.zeros(4, np.float64)
+        _check(lib().fpp_server_stats(self.h, _ptr(v), 4))
+        return dict(launches=int(v[0]), queries=int(v[1]), requests=int(v[2]), waiting=int(v[3]))
+
+    def close(self):
+        if self.h:
+            lib().fpp_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

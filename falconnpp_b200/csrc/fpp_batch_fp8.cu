@@ -1,0 +1,14 @@
+// fpp_batch_fp8.cu — FP8-E4M3-rerank instances of the fused batched kernel.
+#include "fpp_batch_kernel.cuh"
+
+namespace fpp {
+
+KernelSel pick_kernel_fp8(int fht, int d) {
+  const int v = vi_of(d, 16), v32 = vi_of(d, 4);
+  if (v == 1 && v32 == 1) return pick_fht<kRowsFP8, 1, 1>(fht);
+  if (v == 1 && v32 == 2) return pick_fht<kRowsFP8, 1, 2>(fht);
+  if (v == 1 && v32 == 4) return pick_fht<kRowsFP8, 1, 4>(fht);
+  return KernelSel{nullptr, 0};
+}
+
+}  // namespace fpp

@@ -1,0 +1,679 @@
+// fpp_batch_kernel.cuh — the fused batched query kernel k_batch_query and its
+// launch selection, shared by the per-precision translation units
+// (fpp_batch_f32.cu, fpp_batch_bf16.cu, fpp_batch_fp8.cu), which instantiate
+// it for fhtDim 32..512 and d <= 512 and are compiled in parallel.
+#pragma once
+#include <cuda_bf16.h>
+#include <cuda_fp8.h>
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include "fpp_batch.h"
+#include "fpp_device.cuh"
+#include "fpp_rows.cuh"
+
+namespace fpp {
+
+constexpr int kBThreads = 256;
+constexpr int kBWarps = kBThreads / 32;
+constexpr int kBMaxList = 1024;   // L * m entries held in shared memory
+constexpr int kBMaxProbes = 1024;
+constexpr int kBMaxM1 = 16;
+constexpr int kBMaxTop = 1024;    // k * shortlist multiple, and the replay heaps
+constexpr int kHT = 8192;         // shared-memory hash set for the dedupe (2^13 slots)
+constexpr unsigned kHTLimit = kHT - 2048;  // unique ids before switching to the L2 bitset
+constexpr uint32_t kEmpty = 0xffffffffu;
+constexpr int kHistBins = 2048;   // top 11 bits of the score key
+
+struct BatchArgs {
+  const float* Xc;
+  int ld;
+  const unsigned char* Xrows;  // rows reranked first (fp32 = Xc, else bf16/fp8 copy)
+  size_t row_bytes;
+  int nchunk;
+  const float* Xscale;
+  const uint32_t* flips;
+  const uint32_t* bucket_off;
+  const int32_t* ids;
+  int n, d, L, D, log2D;
+  uint32_t NB;
+  const float* Q;
+  int nq;
+  const int* q_k;
+  const int* q_qprobes;
+  int k_uniform, qprobes_uniform;
+  int k_max, qprobes_max;  // per-query values outside [1, max] are rejected
+  int shortlist_mult;
+  int32_t* out;
+  int out_stride;
+  float* out_v;
+  uint32_t* bitset;
+  long long nwords;
+  uint32_t* uniq;
+  uint32_t* score;
+  long long cap;
+  float* gdump;       // [groups][FHT] fallback dumps
+  float* gheap_v;     // [groups][mmax] pair heaps
+  int* gheap_i;
+  int mmax;
+  unsigned int* work;
+  unsigned int* status;  // bit 0: candidate capacity overflow; bit 1: per-query k/qProbes out of range
+};
+
+__device__ __forceinline__ int ceil_sqrt_int(int m) {
+  int r = 0;
+  while (r * r < m) ++r;
+  return r;
+}
+
+// block-wide radix selection of the `want`-th largest key among n keys
+// produced by key_at(i); returns the key; counts of keys >= it in *ge.
+template <typename F>
+__device__ __forceinline__ uint32_t block_select(int n, unsigned want, F key_at, uint32_t* hist, uint32_t* s_pre,
+                                                 uint32_t* s_rem, unsigned* s_cnt, unsigned* ge_out) {
+  if (threadIdx.x == 0) {
+    *s_pre = 0;
+    *s_rem = want;
+  }
+  uint32_t mask = 0;
+  for (int shift = 24; shift >= 0; shift -= 8) {
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) hist[i] = 0;
+    __syncthreads();
+    const uint32_t pre = *s_pre;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      const uint32_t k = key_at(i);
+      if ((k & mask) == pre) atomicAdd(&hist[(k >> shift) & 255u], 1u);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      uint32_t rem = *s_rem;
+      int dg = 255;
+      for (; dg > 0; --dg) {
+        if (hist[dg] >= rem) break;
+        rem -= hist[dg];
+      }
+      *s_pre = pre | ((uint32_t)dg << shift);
+      *s_rem = rem;
+    }
+    mask |= 255u << shift;
+    __syncthreads();
+  }
+  const uint32_t t = *s_pre;
+  if (threadIdx.x == 0) *s_cnt = 0;
+  __syncthreads();
+  unsigned ge = 0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) ge += key_at(i) >= t;
+  atomicAdd(s_cnt, ge);
+  __syncthreads();
+  *ge_out = *s_cnt;
+  __syncthreads();
+  return t;
+}
+
+// ascending bitonic sort of n (<= kBMaxTop) 64-bit keys in shared memory
+__device__ __forceinline__ void block_sort_u64(unsigned long long* a, int n) {
+  int N = 1;
+  while (N < n) N <<= 1;
+  for (int k2 = 2; k2 <= N; k2 <<= 1)
+    for (int j = k2 >> 1; j > 0; j >>= 1) {
+      for (int t = threadIdx.x; t < N / 2; t += blockDim.x) {
+        const int blk = t / j;
+        int lo, hi;
+        if (j == (k2 >> 1)) {
+          lo = blk * k2 + (t - blk * j);
+          hi = blk * k2 + k2 - 1 - (t - blk * j);
+        } else {
+          lo = blk * 2 * j + (t - blk * j);
+          hi = lo + j;
+        }
+        if (hi < n) {
+          const unsigned long long x = a[lo], y = a[hi];
+          if (x > y) {
+            a[lo] = y;
+            a[hi] = x;
+          }
+        }
+      }
+      __syncthreads();
+    }
+}
+
+// dynamic shared memory of k_batch_query (regions reused phase by phase)
+template <int GROUPS>
+struct BatchSmem {
+  static constexpr size_t kHt = 0;                              // hash set (gather)
+  static constexpr size_t kLv = kHt + 4 * kHT;                  // lists (hash, select)
+  static constexpr size_t kLb = kLv + 4 * kBMaxList;
+  static constexpr size_t kProbe = kLb + 4 * kBMaxList;
+  static constexpr size_t kTop = kProbe + 4 * kBMaxProbes;      // sorted (key, id) of the top-k stage
+  static constexpr size_t kGv = kTop + 8 * kBMaxTop;
+  static constexpr size_t kGc = kGv + 4 * GROUPS * 2 * (kBMaxM1 + 1);
+  static constexpr size_t kRhv = kGc + 4 * GROUPS * 2 * (kBMaxM1 + 1);
+  static constexpr size_t kRhi = kRhv + 4 * GROUPS * kBMaxM1;
+  static constexpr size_t kQ = kRhi + 4 * GROUPS * kBMaxM1;
+  static constexpr size_t kBytes = kQ + 4 * 1024;
+  uint32_t* ht;
+  float* lv;
+  uint32_t* lb;
+  uint32_t* probe;
+  unsigned long long* top;
+  float* gv;
+  int* gc;
+  float* rhv;
+  int* rhi;
+  float* q;  // the current query, zero padded to 1024 floats
+  // aliases: gather prefix arrays over the lists; the score histogram over
+  // both lists (2048 u32); the probe-cut replay heap in the top region; the
+  // re-score arrays and the final replay heap in the hash-set region
+  __device__ uint32_t* po() const { return lb; }
+  __device__ uint32_t* pe() const { return reinterpret_cast<uint32_t*>(lv); }
+  __device__ uint32_t* hist() const { return reinterpret_cast<uint32_t*>(lv); }
+  __device__ float* phv() const { return reinterpret_cast<float*>(top); }
+  __device__ int* phi() const { return reinterpret_cast<int*>(top) + 512; }
+  __device__ uint32_t* sid() const { return ht; }
+  __device__ uint32_t* ssc() const { return ht + 1024; }
+  __device__ float* fhv() const { return reinterpret_cast<float*>(ht + 2048); }
+  __device__ int* fhi() const { return reinterpret_cast<int*>(ht + 3072); }
+  __device__ explicit BatchSmem(unsigned char* p)
+      : ht(reinterpret_cast<uint32_t*>(p + kHt)),
+        lv(reinterpret_cast<float*>(p + kLv)),
+        lb(reinterpret_cast<uint32_t*>(p + kLb)),
+        probe(reinterpret_cast<uint32_t*>(p + kProbe)),
+        top(reinterpret_cast<unsigned long long*>(p + kTop)),
+        gv(reinterpret_cast<float*>(p + kGv)),
+        gc(reinterpret_cast<int*>(p + kGc)),
+        rhv(reinterpret_cast<float*>(p + kRhv)),
+        rhi(reinterpret_cast<int*>(p + kRhi)),
+        q(reinterpret_cast<float*>(p + kQ)) {}
+};
+
+template <int FHT>
+constexpr size_t batch_smem_bytes() {
+  return BatchSmem<kBThreads / Geo<FHT>::G>::kBytes;
+}
+
+__device__ __forceinline__ uint32_t ht_slot(uint32_t id) { return (id * 2654435761u) >> (32 - 13); }
+
+template <int FHT, int MODE, int VI, int VI32>
+__global__ void __launch_bounds__(kBThreads, 3) k_batch_query(BatchArgs a) {
+  constexpr int E = Geo<FHT>::E;
+  constexpr int G = Geo<FHT>::G;
+  constexpr int WORDS = Geo<FHT>::WORDS;
+  constexpr int GROUPS = kBThreads / G;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  BatchSmem<GROUPS> sm(smem_raw);
+  float* s_lv = sm.lv;
+  uint32_t* s_lb = sm.lb;
+  uint32_t* s_probe = sm.probe;
+  unsigned long long* s_top = sm.top;
+  __shared__ uint32_t hist[256];
+  __shared__ uint32_t s_pre, s_rem;
+  __shared__ unsigned s_cnt, s_u, s_sel, s_q, s_ovf, s_bstar, s_above;
+  __shared__ long long tmp[32];
+
+  const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  const int warp = tid >> 5;
+  const int gl = lane & (G - 1);
+  const int grp = tid / G;
+  const unsigned gmask = (G == 32) ? kFullMask : (((1u << G) - 1u) << (lane & ~(G - 1)));
+  const long long gid = (long long)blockIdx.x * GROUPS + grp;
+  uint32_t* bits = a.bitset + (size_t)blockIdx.x * a.nwords;
+  uint32_t* uq = a.uniq + (size_t)blockIdx.x * a.cap;
+  uint32_t* sc = a.score + (size_t)blockIdx.x * a.cap;
+  float* ydump = a.gdump + gid * FHT;
+  float* ph_v = a.gheap_v + gid * (long long)a.mmax;
+  int* ph_i = a.gheap_i + gid * (long long)a.mmax;
+  const int L = a.L;
+  for (int i = tid; i < kHT; i += kBThreads) sm.ht[i] = kEmpty;
+
+  for (;;) {
+    __syncthreads();
+    if (tid == 0) s_q = atomicAdd(a.work, 1u);
+    __syncthreads();
+    const unsigned qu = s_q;
+    if (qu >= (unsigned)a.nq) break;
+    const int q = (int)qu;
+    const int k = a.q_k ? a.q_k[q] : a.k_uniform;
+    const int Qp = a.q_qprobes ? a.q_qprobes[q] : a.qprobes_uniform;
+    if (k < 1 || k > a.k_max || Qp < 1 || Qp > a.qprobes_max) {  // block-uniform
+      if (tid == 0) atomicOr(a.status, 2u);
+      for (int j = tid; j < a.out_stride; j += kBThreads) a.out[(size_t)q * a.out_stride + j] = -1;
+      continue;
+    }
+    const int m = (2 * Qp + L - 1) / L;  // ceil(2.0 * qProbes / L), FalconnPP.cpp:336
+    const int m1 = ceil_sqrt_int(m);     // ceil(sqrt(m)), FalconnPP.cpp:337
+    const int M = L * m;
+    const float* qv = a.Q + (size_t)q * a.d;
+    for (int i = tid; i < 1024; i += kBThreads) sm.q[i] = i < a.d ? qv[i] : 0.0f;
+
+    // ---- 1. rotate + hash every table (FalconnPP.cpp:358-531)
+    {
+      float xr[E];
+#pragma unroll
+      for (int e = 0; e < E; ++e) {
+        const int idx = gl * E + e;
+        xr[e] = idx < a.d ? __ldg(qv + idx) : 0.0f;
+      }
+      const int cnt = min(m1 + 1, a.D);
+      const int rounds = (L + GROUPS - 1) / GROUPS;
+      for (int rd = 0; rd < rounds; ++rd) {
+        const int l = rd * GROUPS + grp;
+        const bool active = l < L;
+        const int lt = active ? l : 0;
+#pragma unroll 1
+        for (int layer = 0; layer < 2; ++layer) {
+          float y[E];
+#pragma unroll
+          for (int e = 0; e < E; ++e) y[e] = xr[e];
+          hd3_rotate<FHT>(y, a.flips + ((size_t)(layer * L + lt) * 3) * WORDS, gl);
+          float* lv = sm.gv + (grp * 2 + layer) * (kBMaxM1 + 1);
+          int* lc = sm.gc + (grp * 2 + layer) * (kBMaxM1 + 1);
+          const int f = group_top_cp_auto<FHT>(y, gl, a.D, a.log2D, cnt, lv, lc);
+          __syncwarp();
+          bool ok = (f == cnt);
+          for (int t = 1; t < cnt; ++t)
+            if (ok && !(lv[t - 1] > lv[t])) ok = false;
+          if (!ok) {
+#pragma unroll
+            for (int e = 0; e < E; ++e) ydump[gl * E + e] = y[e];
+            __syncwarp(gmask);
+            if (gl == 0) replay_layer_topp(ydump, a.D, a.log2D, m1, sm.rhv + grp * kBMaxM1, sm.rhi + grp * kBMaxM1, lv, lc);
+            __syncwarp(gmask);
+          }
+        }
+        if (gl == 0 && active) {
+          const float* lv1 = sm.gv + (grp * 2 + 0) * (kBMaxM1 + 1);
+          const int* lc1 = sm.gc + (grp * 2 + 0) * (kBMaxM1 + 1);
+          const float* lv2 = sm.gv + (grp * 2 + 1) * (kBMaxM1 + 1);
+          const int* lc2 = sm.gc + (grp * 2 + 1) * (kBMaxM1 + 1);
+          const uint32_t tbase = (uint32_t)l * a.NB;
+          const int twoD = 2 * a.D;
+          if (m == 1) {
+            s_lv[l] = __fadd_rn(lv1[0], lv2[0]);
+            s_lb[l] = tbase + (uint32_t)(lc1[0] * twoD + lc2[0]);
+          } else {
+            int hn = 0;
+            for (int i = 0; i < m1; ++i)
+              for (int j = 0; j < m1; ++j)
+                topp_offer<int>(ph_v, ph_i, hn, m, __fadd_rn(lv1[i], lv2[j]), lc1[i] * twoD + lc2[j]);
+            for (int j = m - 1; j >= 0; --j) {
+              s_lv[l * m + j] = ph_v[0];
+              s_lb[l * m + j] = tbase + (uint32_t)ph_i[0];
+              heap_pop<true, int>(ph_v, ph_i, hn);
+            }
+          }
+        }
+        __syncwarp();
+      }
+    }
+    __syncthreads();
+
+    // ---- 2. global top-qProbes of the L*m lists (FalconnPP.cpp:540-582):
+    // rank by counting; a tie straddling the cut replays the reference's heap
+    {
+      long long run = 0;
+      bool tie = false;
+      for (int base = 0; base < M; base += kBThreads) {
+        const int i = base + tid;
+        bool take = false;
+        if (i < M) {
+          const uint32_t ki = ord_key(s_lv[i]);
+          int gt = 0, eq = 0;
+          for (int j = 0; j < M; ++j) {
+            const uint32_t kj = ord_key(s_lv[j]);
+            gt += kj > ki;
+            eq += kj == ki;
+          }
+          take = gt < Qp;
+          tie |= take && gt + eq > Qp;
+        }
+        long long tot;
+        const long long pos = block_exclusive_scan(take ? 1 : 0, tmp, &tot) + run;
+        if (take && pos < Qp) s_probe[pos] = s_lb[i];
+        run += tot;
+      }
+      if (__syncthreads_or(tie) && tid == 0) {
+        float* hv = sm.phv();
+        int* hi = sm.phi();
+        int* track = hi + L;
+        int n = 0;
+        for (int l = 0; l < L; ++l) {
+          heap_push<false, int>(hv, hi, n, s_lv[l * m], l * m);
+          track[l] = 0;
+        }
+        for (int pc = 0; pc < Qp; ++pc) {
+          const int pos = hi[0];
+          heap_pop<false, int>(hv, hi, n);
+          s_probe[pc] = s_lb[pos];
+          const int tb = pos / m;
+          track[tb]++;
+          if (track[tb] < m) heap_push<false, int>(hv, hi, n, s_lv[tb * m + track[tb]], tb * m + track[tb]);
+        }
+      }
+      __syncthreads();
+    }
+
+    // ---- 3. gather + dedupe (FalconnPP.cpp:584-606): the candidates of all
+    // probes flattened over the warps; dedupe in a shared-memory hash set, or
+    // (when a query has too many unique ids) in the block's L2 bitset
+    uint32_t* s_po = sm.po();
+    uint32_t* s_pe = sm.pe();
+    {
+      long long run = 0;
+      for (int base = 0; base < Qp; base += kBThreads) {
+        const int p = base + tid;
+        uint32_t o = 0, sz = 0;
+        if (p < Qp) {
+          const uint32_t g = s_probe[p];
+          o = a.bucket_off[g];
+          sz = a.bucket_off[g + 1] - o;
+        }
+        long long tot;
+        const long long ex = block_exclusive_scan((long long)sz, tmp, &tot) + run;
+        if (p < Qp) {
+          s_po[p] = o;
+          s_pe[p] = (uint32_t)(ex + sz);
+        }
+        run += tot;
+      }
+    }
+    if (tid == 0) {
+      s_u = 0;
+      s_ovf = 0;
+    }
+    __syncthreads();
+    const uint32_t C = s_pe[Qp - 1];
+    const unsigned cap = (unsigned)a.cap;
+    bool use_bitset = false;
+    for (int pass = 0; pass < 2; ++pass) {
+      const uint32_t per = (((C + kBWarps - 1) / kBWarps) + 127u) & ~127u;
+      const uint32_t c_begin = min(C, (uint32_t)warp * per);
+      const uint32_t c_end = min(C, c_begin + per);
+      int cur = 0;
+      {
+        int lo = 0, hi = Qp - 1;
+        while (lo < hi) {
+          const int mid = (lo + hi) >> 1;
+          if (s_pe[mid] > c_begin) hi = mid; else lo = mid + 1;
+        }
+        cur = lo;
+      }
+      for (uint32_t c0 = c_begin; c0 < c_end; c0 += 128u) {
+        if (!use_bitset && *(volatile unsigned*)&s_ovf) break;
+        uint32_t idv[4];
+#pragma unroll
+        for (int h = 0; h < 4; ++h) {
+          const uint32_t i = c0 + h * 32 + lane;
+          idv[h] = kEmpty;
+          if (i < c_end) {
+            int p = cur;
+            while (s_pe[p] <= i) ++p;
+            const uint32_t st = p > 0 ? s_pe[p - 1] : 0u;
+            idv[h] = (uint32_t)__ldg(a.ids + s_po[p] + (i - st));
+          }
+        }
+        {
+          const uint32_t nxt = min(c0 + 128u, c_end - 1);
+          while (cur < Qp - 1 && s_pe[cur] <= nxt) ++cur;
+        }
+        bool fresh[4];
+#pragma unroll
+        for (int h = 0; h < 4; ++h) {
+          fresh[h] = false;
+          const uint32_t id = idv[h];
+          if (id != kEmpty) {
+            if (use_bitset) {
+              const uint32_t bit = 1u << (id & 31u);
+              fresh[h] = (atomicOr(bits + (id >> 5), bit) & bit) == 0u;
+            } else {
+              // linear probing; the table never holds more than kHTLimit +
+              // 1024 ids, so an empty slot always exists
+              uint32_t slot = ht_slot(id);
+              for (;;) {
+                const uint32_t old = atomicCAS(sm.ht + slot, kEmpty, id);
+                if (old == kEmpty) {
+                  fresh[h] = true;
+                  break;
+                }
+                if (old == id) break;
+                slot = (slot + 1) & (kHT - 1);
+              }
+            }
+          }
+        }
+#pragma unroll
+        for (int h = 0; h < 4; ++h) {
+          const unsigned bal = __ballot_sync(kFullMask, fresh[h]);
+          if (bal) {
+            unsigned base = 0;
+            if (lane == 0) base = atomicAdd(&s_u, (unsigned)__popc(bal));
+            base = __shfl_sync(kFullMask, base, 0);
+            const unsigned pos = base + __popc(bal & ((1u << lane) - 1u));
+            if (fresh[h] && pos < cap) uq[pos] = idv[h];
+          }
+        }
+        if (!use_bitset && lane == 0 && *(volatile unsigned*)&s_u >= kHTLimit) s_ovf = 1u;
+      }
+      __syncthreads();
+      if (use_bitset || !s_ovf) break;
+      // too many unique ids for the hash set: start over with the bitset
+      for (int i = tid; i < kHT; i += kBThreads) sm.ht[i] = kEmpty;
+      if (tid == 0) s_u = 0;
+      use_bitset = true;
+      __syncthreads();
+    }
+    const unsigned U = s_u;
+    int32_t* orow = a.out + (size_t)q * a.out_stride;
+    float* ovrow = a.out_v ? a.out_v + (size_t)q * a.out_stride : nullptr;
+    if (U > cap) {
+      if (tid == 0) atomicOr(a.status, 1u);
+      for (int j = tid; j < k; j += kBThreads) {
+        orow[j] = -1;
+        if (ovrow) ovrow[j] = 0.0f;
+      }
+      for (long long w = tid; w < a.nwords; w += kBThreads) bits[w] = 0u;
+      for (int i = tid; i < kHT; i += kBThreads) sm.ht[i] = kEmpty;
+      continue;
+    }
+
+    // ---- 4. rerank the unique rows (FalconnPP.cpp:642-660), with a
+    // histogram of the scores' top 11 key bits for the selection below
+    uint32_t* s_hist = sm.hist();
+    for (int i = tid; i < kHistBins; i += kBThreads) s_hist[i] = 0u;
+    __syncthreads();
+    {
+      const float* scl = MODE == kRowsFP8 ? a.Xscale : nullptr;
+      rerank_rows<MODE, VI, (MODE == kRowsF32 ? 2 : 4)>(uq, U, sc, sm.q, a.Xrows, a.row_bytes, a.nchunk, scl,
+                                                           warp, kBWarps, lane, s_hist);
+    }
+    __syncthreads();
+
+    // ---- 5. shortlist by the first scores, exact FP32 re-score, top-k
+    const unsigned kk = (unsigned)k;
+    const unsigned R = MODE == kRowsF32 ? kk : min((unsigned)kBMaxTop, kk * (unsigned)a.shortlist_mult);
+    unsigned nsel = U;
+    bool exact = true;
+    if (U > R) {
+      // the bin holding the R-th largest key: thread t owns bins
+      // [2048 - 8(t+1), 2048 - 8t), scanned from the top
+      {
+        uint32_t c[8];
+        uint32_t sum = 0;
+        const int hi = kHistBins - 8 * tid;
+#pragma unroll
+        for (int b = 0; b < 8; ++b) {
+          c[b] = s_hist[hi - 1 - b];
+          sum += c[b];
+        }
+        long long tot;
+        const long long above = block_exclusive_scan((long long)sum, tmp, &tot);
+        if (above < (long long)R && above + sum >= R) {
+          long long cum = above;
+#pragma unroll
+          for (int b = 0; b < 8; ++b) {
+            if (cum + c[b] >= R && cum < (long long)R) {
+              s_bstar = (uint32_t)(hi - 1 - b);
+              s_above = (uint32_t)(cum + c[b]);
+            }
+            cum += c[b];
+          }
+        }
+      }
+      __syncthreads();
+      const uint32_t bstar = s_bstar;
+      if (s_above <= (unsigned)kBMaxTop) {
+        if (tid == 0) s_sel = 0;
+        __syncthreads();
+        for (unsigned i = tid; i < U; i += kBThreads) {
+          const uint32_t key = ord_key_bits(sc[i]);
+          if ((key >> 21) >= bstar) {
+            const unsigned pos = atomicAdd(&s_sel, 1u);
+            s_top[pos] = ((unsigned long long)(~key) << 32) | uq[i];
+          }
+        }
+        __syncthreads();
+        nsel = s_sel;
+      } else {
+        // very many equal top bits: radix selection of the R-th key
+        unsigned ge;
+        const uint32_t t = block_select((int)U, R, [&](int i) { return ord_key_bits(sc[i]); }, hist, &s_pre,
+                                        &s_rem, &s_cnt, &ge);
+        if (MODE == kRowsF32 && ge != R) {
+          exact = false;
+        } else {
+          if (tid == 0) s_sel = 0;
+          __syncthreads();
+          for (unsigned i = tid; i < U; i += kBThreads) {
+            const uint32_t key = ord_key_bits(sc[i]);
+            if (key >= t) {
+              const unsigned pos = atomicAdd(&s_sel, 1u);
+              if (pos < (unsigned)kBMaxTop) s_top[pos] = ((unsigned long long)(~key) << 32) | uq[i];
+            }
+          }
+          __syncthreads();
+          nsel = min(s_sel, (unsigned)kBMaxTop);
+        }
+      }
+    } else {
+      for (unsigned i = tid; i < U; i += kBThreads)
+        s_top[i] = ((unsigned long long)(~ord_key_bits(sc[i])) << 32) | uq[i];
+      __syncthreads();
+    }
+    if (exact) {
+      block_sort_u64(s_top, (int)nsel);
+      if (MODE != kRowsF32) {
+        // exact FP32 re-score of the best R with the parity dot order
+        nsel = min(nsel, R);
+        uint32_t* sid = sm.sid();
+        uint32_t* ssc = sm.ssc();
+        for (unsigned i = tid; i < nsel; i += kBThreads) sid[i] = (uint32_t)s_top[i];
+        __syncthreads();
+        rerank_rows<kRowsF32, VI32>(sid, nsel, ssc, sm.q, reinterpret_cast<const unsigned char*>(a.Xc),
+                                    (size_t)a.ld * 4, a.ld / 4, nullptr, warp, kBWarps, lane, nullptr);
+        __syncthreads();
+        for (unsigned i = tid; i < nsel; i += kBThreads)
+          s_top[i] = ((unsigned long long)(~ord_key_bits(ssc[i])) << 32) | sid[i];
+        __syncthreads();
+        block_sort_u64(s_top, (int)nsel);
+      }
+      const unsigned kept = min(nsel, kk);
+      unsigned dup = 0;
+      // equal FP32 scores in the kept list, or at the k-th place: heap order decides
+      for (unsigned i = tid; i + 1 < nsel && i < kk; i += kBThreads) dup |= (s_top[i] >> 32) == (s_top[i + 1] >> 32);
+      exact = !__syncthreads_or(dup);
+      if (exact) {
+        for (int j = tid; j < k; j += kBThreads) {
+          if ((unsigned)j < kept) {
+            orow[j] = (int32_t)(uint32_t)s_top[j];
+            if (ovrow) ovrow[j] = __uint_as_float(ord_key_inv_dev(~(uint32_t)(s_top[j] >> 32)));
+          } else {
+            orow[j] = 0;
+            if (ovrow) ovrow[j] = 0.0f;
+          }
+        }
+      }
+    }
+    bool bits_dirty = use_bitset;
+    if (!exact) {
+      // the reference's min-heap over the candidates in ascending id order
+      // (FalconnPP.cpp:633-673): all of them in FP32 mode, the shortlist otherwise
+      const bool whole = (MODE == kRowsF32);
+      const unsigned nc = whole ? U : nsel;
+      uint32_t* cid = uq;
+      uint32_t* csc = sc;
+      if (!whole) {
+        for (unsigned i = tid; i < nc; i += kBThreads) {
+          cid[i] = (uint32_t)s_top[i];
+          csc[i] = ord_key_inv_dev(~(uint32_t)(s_top[i] >> 32));
+        }
+        __syncthreads();
+        if (use_bitset) {  // the unique list was overwritten: clear every word
+          for (long long w = tid; w < a.nwords; w += kBThreads) bits[w] = 0u;
+          bits_dirty = false;
+        }
+      }
+      block_bitonic_sort_u32(cid, csc, (int)nc);
+      if (tid == 0) {
+        float* hv = sm.fhv();
+        int* hi = sm.fhi();
+        int n = 0;
+        for (unsigned i = 0; i < nc; ++i) topp_offer<int>(hv, hi, n, k, __uint_as_float(csc[i]), (int)cid[i]);
+        for (int j = n; j < k; ++j) {
+          orow[j] = 0;
+          if (ovrow) ovrow[j] = 0.0f;
+        }
+        for (int j = n - 1; j >= 0; --j) {
+          orow[j] = hi[0];
+          if (ovrow) ovrow[j] = hv[0];
+          heap_pop<true, int>(hv, hi, n);
+        }
+      }
+      __syncthreads();
+    }
+    // ---- 6. leave the hash set empty and the bitset clear
+    for (int i = tid; i < kHT; i += kBThreads) sm.ht[i] = kEmpty;
+    if (bits_dirty)
+      for (unsigned i = tid; i < U; i += kBThreads) bits[uq[i] >> 5] = 0u;
+  }
+}
+
+
+struct KernelSel {
+  const void* fn;
+  size_t smem;
+};
+
+template <int FHT, int MODE, int VI, int VI32>
+static KernelSel kernel_ptr() {
+  const void* fn = reinterpret_cast<const void*>(&k_batch_query<FHT, MODE, VI, VI32>);
+  const size_t smem = batch_smem_bytes<FHT>();
+  cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  return KernelSel{fn, smem};
+}
+
+template <int MODE, int VI, int VI32>
+static KernelSel pick_fht(int fht) {
+  switch (fht) {
+    case 32: return kernel_ptr<32, MODE, VI, VI32>();
+    case 64: return kernel_ptr<64, MODE, VI, VI32>();
+    case 128: return kernel_ptr<128, MODE, VI, VI32>();
+    case 256: return kernel_ptr<256, MODE, VI, VI32>();
+    case 512: return kernel_ptr<512, MODE, VI, VI32>();
+    default: return KernelSel{nullptr, 0};
+  }
+}
+
+// per-precision selection (VI: 16-byte chunks per virtual lane of the first
+// rerank; VI32: of the FP32 rows), defined in fpp_batch_{f32,bf16,fp8}.cu
+KernelSel pick_kernel_f32(int fht, int d);
+KernelSel pick_kernel_bf16(int fht, int d);
+KernelSel pick_kernel_fp8(int fht, int d);
+
+inline int vi_of(int d, int epc) {
+  const int v = ((d + epc - 1) / epc + 31) / 32;
+  return v <= 1 ? 1 : v <= 2 ? 2 : 4;
+}
+
+}  // namespace fpp

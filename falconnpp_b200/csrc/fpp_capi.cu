@@ -414,6 +414,121 @@ int fpp_set_query_form(fpp_index* h, int form, int precision, int shortlist_mult
   return ok();
 }
 
+int fpp_autotune(fpp_index* h, const float* d_queries, int n_queries, int k, double min_agreement, double* report,
+                 void* stream) {
+  if (!h) return fail(FPP_ERR_INVALID_ARGUMENT, "autotune: NULL handle");
+  std::lock_guard<std::mutex> g(h->mu);
+  if (!h->built) return fail(FPP_ERR_NOT_BUILT, "autotune: the index is not built");
+  if (n_queries < 1 || k < 1 || k > 1024 || !d_queries)
+    return fail(FPP_ERR_INVALID_ARGUMENT, "autotune: need queries and 1 <= k <= 1024");
+  if (use_device(h)) return FPP_ERR_CUDA;
+  cudaStream_t s = stream ? (cudaStream_t)stream : h->stream;
+  const size_t nout = (size_t)n_queries * k;
+  int32_t* d_ref = nullptr;
+  int32_t* d_out = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (cudaMalloc(&d_ref, sizeof(int32_t) * nout) != cudaSuccess ||
+      cudaMalloc(&d_out, sizeof(int32_t) * nout) != cudaSuccess) {
+    cudaFree(d_ref);
+    return fail(FPP_ERR_OUT_OF_MEMORY, "autotune: cannot allocate result buffers");
+  }
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  std::vector<int32_t> ref(nout), got(nout);
+  auto run = [&](int precision, int mult, int bps, int32_t* out, float* ms) -> int {
+    fpp::BatchRequest rq;
+    rq.Q = d_queries;
+    rq.nq = n_queries;
+    rq.k_uniform = k;
+    rq.qprobes_uniform = h->P.qProbes;
+    rq.k_max = k;
+    rq.qprobes_max = h->P.qProbes;
+    rq.mode = precision;
+    rq.shortlist_mult = mult;
+    rq.out = out;
+    rq.out_stride = k;
+    rq.blocks_per_sm = bps;
+    rq.check_status = true;
+    fpp::BatchResult res;
+    fpp::Error err{0, ""};
+    int rc = fpp::batch_query(h->P, h->di, h->bw, rq, s, res, err);  // warm-up, checks status
+    if (rc) return fail(rc, err.msg);
+    if (res.overflow || res.bad_params) return fail(FPP_ERR_UNSUPPORTED, "autotune: batch did not complete");
+    float best = 1e30f;
+    rq.check_status = false;
+    for (int rep = 0; rep < 3; ++rep) {
+      cudaEventRecord(e0, s);
+      rc = fpp::batch_query(h->P, h->di, h->bw, rq, s, res, err);
+      cudaEventRecord(e1, s);
+      if (rc) return fail(rc, err.msg);
+      cudaEventSynchronize(e1);
+      float t = 0;
+      cudaEventElapsedTime(&t, e0, e1);
+      best = std::min(best, t);
+    }
+    *ms = best;
+    return FPP_OK;
+  };
+  float ms = 0;
+  int rc = run(0, 1, 0, d_ref, &ms);
+  double best_ms = 1e30, best_agree = 0;
+  int best_bps = 0, best_prec = 0, best_mult = 4, tried = 0;
+  if (rc == FPP_OK) {
+    cudaMemcpy(ref.data(), d_ref, sizeof(int32_t) * nout, cudaMemcpyDeviceToHost);
+    best_ms = ms;
+    best_agree = 1.0;
+    const int precs[2] = {1, 2};
+    const int mults[3] = {1, 2, 4};
+    const int bpss[3] = {1, 2, 3};
+    for (int pi = 0; pi < 2 && rc == FPP_OK; ++pi)
+      for (int mi = 0; mi < 3 && rc == FPP_OK; ++mi)
+        for (int bi = 0; bi < 3 && rc == FPP_OK; ++bi) {
+          if ((long long)k * mults[mi] > 1024) continue;
+          rc = run(precs[pi], mults[mi], bpss[bi], d_out, &ms);
+          if (rc) break;
+          ++tried;
+          cudaMemcpy(got.data(), d_out, sizeof(int32_t) * nout, cudaMemcpyDeviceToHost);
+          long long hit = 0;
+          for (int q = 0; q < n_queries; ++q) {
+            const int32_t* a = &ref[(size_t)q * k];
+            const int32_t* b = &got[(size_t)q * k];
+            for (int i = 0; i < k; ++i)
+              for (int j = 0; j < k; ++j)
+                if (a[i] == b[j]) {
+                  ++hit;
+                  break;
+                }
+          }
+          const double agree = (double)hit / (double)nout;
+          if (agree >= min_agreement && ms < best_ms) {
+            best_ms = ms;
+            best_agree = agree;
+            best_bps = bpss[bi];
+            best_prec = precs[pi];
+            best_mult = mults[mi];
+          }
+        }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(d_ref);
+  cudaFree(d_out);
+  if (rc) return rc;
+  h->form = 1;
+  h->precision = best_prec;
+  h->shortlist_mult = best_mult;
+  h->blocks_per_sm = best_bps;
+  if (report) {
+    report[0] = best_ms;
+    report[1] = best_bps;
+    report[2] = best_prec;
+    report[3] = best_mult;
+    report[4] = best_agree;
+    report[5] = tried;
+  }
+  return ok();
+}
+
 int fpp_query_batched(fpp_index* h, const float* d_queries, int n_queries, const int32_t* d_k,
                       const int32_t* d_qprobes, int k_max, int qprobes_max, int32_t* d_out, int out_stride,
                       float* d_out_val, void* stream) {

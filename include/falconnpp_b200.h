@@ -158,6 +158,40 @@ int fpp_query_batched(fpp_index* h, const float* d_queries, int n_queries, const
                       const int32_t* d_qprobes, int k_max, int qprobes_max, int32_t* d_out, int out_stride,
                       float* d_out_val, void* stream);
 
+/* Autotuner of the batched form (no reference counterpart).  On a sample of
+ * device queries it times the fused kernel over blocks per SM {1,2,3},
+ * precision {BF16, FP8} and shortlist multiple {1,2,4}, against the FP32
+ * exact batched result (occupancy-limited blocks per SM), and keeps the
+ * fastest configuration whose top-k ids agree with the exact ones on at least
+ * min_agreement of the ids (the FP32 configuration itself when none does).
+ * The handle is switched to the batched form with that configuration.
+ * report (may be NULL): double[6] = best ms for the sample, blocks per SM
+ * (0 = occupancy limit), precision, shortlist multiple, agreement,
+ * configurations tried. */
+int fpp_autotune(fpp_index* h, const float* d_queries, int n_queries, int k, double min_agreement, double* report,
+                 void* stream);
+
+/* Serving loop with continuous batching (no reference counterpart).
+ * A worker thread packs submitted requests (1..max_batch queries each, their
+ * own k <= k_max and qProbes <= qprobes_max) into mixed batches of the
+ * batched form and launches them on n_streams concurrent streams; requests
+ * that arrive while batches run are admitted as stream slots free up, as
+ * long as the queries and results in flight stay within
+ * memory_budget_bytes (a request is always admitted into an empty slot).
+ * Uses the handle's precision and shortlist setting at creation; do not
+ * rebuild or clear the index while a server exists.  queries / out are host
+ * buffers that must stay valid until fpp_server_wait returns for the ticket;
+ * wait on each ticket exactly once.  latency_ms: submit to results written. */
+typedef struct fpp_server fpp_server;
+int fpp_server_create(fpp_index* h, int n_streams, long long memory_budget_bytes, int max_batch, int k_max,
+                      int qprobes_max, fpp_server** out);
+int fpp_server_submit(fpp_server* s, const float* queries, int n_queries, int k, int qprobes, int32_t* out,
+                      long long* ticket);
+int fpp_server_wait(fpp_server* s, long long ticket, double* latency_ms);
+/* out[0] launches, out[1] queries, out[2] requests submitted, out[3] requests waiting. */
+int fpp_server_stats(fpp_server* s, double* out, int n);
+void fpp_server_destroy(fpp_server* s);
+
 /* No counterpart in the reference.  The gather, deduplicate, rerank and top-k
  * stage of fpp_query for callers that cannot allocate device memory: code
  * recording a CUDA graph, a serving thread that must not stall on cudaMalloc /
