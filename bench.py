@@ -416,17 +416,268 @@ def run_reference(args, w):
     }
 
 
+# ---------------------------------------------------------------- the other configurations
+# Single-GPU measurements of the precision, batching and serving forms.  They
+# print their own JSON line and are not the headline (the default workload is).
+
+PRECISION_10M = dict(n=10_000_000, d=128, n_centres=4096, norm_sigma=0.5, L=128, D=128, minSize=50, alpha=0.01,
+                     iProbes=3, nq=10_000, k=10, qprobes=40)
+
+
+def _build_index(w, X):
+    import torch
+    from falconnpp_b200 import capi
+    idx = capi.Index(w["n"], w["d"])
+    idx.set_index_param(w["L"], w["D"], w["minSize"], w["alpha"], w["iProbes"], 8, INDEX_SEED)
+    Xd = torch.from_numpy(X).cuda()
+    t0 = time.perf_counter()
+    idx.build_device(Xd.data_ptr(), torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    return idx, Xd, time.perf_counter() - t0
+
+
+def _time_batched(idx, Qd, nq, k, qp, out, stream, steps, warmup, val=None):
+    import torch
+    for _ in range(warmup):
+        idx.query_batched(Qd.data_ptr(), nq, None, None, k, qp, out.data_ptr(), k,
+                          val.data_ptr() if val is not None else None, stream.cuda_stream)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        e0.record()
+        for _ in range(steps):
+            idx.query_batched(Qd.data_ptr(), nq, None, None, k, qp, out.data_ptr(), k,
+                              val.data_ptr() if val is not None else None, stream.cuda_stream)
+        e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def run_precision(args):
+    """n=10M, d=128, 4,096-centre mixture with log-normal(0, 0.5) norms; L=128,
+    n_proj=128, iProbes=3, qProbes=40, k=10.  BF16 and FP8-E4M3 (per-row scale)
+    rerank + FP32 re-score of a 4k shortlist, against the plain FP32 path.
+    Reports recall@10 and dot-product errors against FP64 (bucket_minSize=50,
+    alpha=0.01: the configuration does not name them)."""
+    import torch
+    from falconnpp_b200 import synth
+    w = PRECISION_10M
+    X = synth.mixture(w["n"], w["d"], n_centres=w["n_centres"], norm_sigma=w["norm_sigma"], seed=0)
+    Q = synth.mixture(w["nq"], w["d"], n_centres=w["n_centres"], norm_sigma=w["norm_sigma"], seed=1)
+    idx, Xd, build_s = _build_index(w, X)
+    k, qp, nq = w["k"], w["qprobes"], w["nq"]
+    idx.set_qprobes(qp)
+    ns = 300
+    truth = exact_topk_fp64(Xd, Q[:ns], k)
+    Qd = torch.from_numpy(Q).cuda()
+    out = torch.zeros((nq, k), dtype=torch.int32, device="cuda")
+    val = torch.zeros((nq, k), dtype=torch.float32, device="cuda")
+    stream = torch.cuda.Stream()
+    center = torch.from_numpy(idx.dump_center()).cuda()
+    Xc64 = (Xd - center).double()
+    forms = {}
+    for name, (form, prec, mult) in {"plain-fp32": (0, 0, 4), "batched-bf16": (1, 1, 4),
+                                     "batched-fp8": (1, 2, 4)}.items():
+        idx.set_query_form(form, prec, mult)
+        if form == 0:
+            idx.query_device(Qd.data_ptr(), nq, k, out.data_ptr(), stream.cuda_stream)
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            with torch.cuda.stream(stream):
+                e0.record()
+                for _ in range(args.steps):
+                    idx.query_device(Qd.data_ptr(), nq, k, out.data_ptr(), stream.cuda_stream)
+                e1.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / args.steps
+        else:
+            ms = _time_batched(idx, Qd, nq, k, qp, out, stream, args.steps, args.warmup, val)
+        ids = out.cpu().numpy()
+        r = {"value": round(nq / (ms / 1000.0), 1), "ms_per_step": round(ms, 4),
+             "recall_at_10": round(recall(truth, ids[:ns], k), 4)}
+        if form == 1:
+            # returned FP32 scores against FP64 dots of the same (query, id) pairs
+            qi = torch.from_numpy(Q[:ns]).cuda().double()
+            idt = torch.from_numpy(ids[:ns]).cuda().long()
+            exact = (Xc64[idt] * qi[:, None, :]).sum(-1)
+            err = (val[:ns].double() - exact).abs()
+            r["max_abs_err_returned_fp32"] = float(err.max())
+            # error of the low-precision row copies alone on the same pairs
+            rows = Xc64[idt].float()
+            if prec == 1:
+                lp = rows.bfloat16().double()
+            else:
+                sc = rows.abs().amax(-1, keepdim=True) / 448.0
+                sc = torch.where(sc > 0, sc, torch.ones_like(sc))
+                lp = (rows / sc).to(torch.float8_e4m3fn).double() * sc.double()
+            lpd = (lp * qi[:, None, :]).sum(-1)
+            r["max_abs_err_lowp_dot"] = float((lpd - exact).abs().max())
+            r["max_rel_err_lowp_dot"] = float(((lpd - exact).abs() / exact.abs().clamp_min(1e-12)).max())
+        forms[name] = r
+    return {"workload": "precision-10Mx128", "config": {k2: v for k2, v in w.items()}, "build_s": round(build_s, 2),
+            "forms": forms, "data": "synthetic", "unit": "queries/s"}
+
+
+def run_mixed(args):
+    """The 1M x 200 index queried with 65,536 queries in uneven batches (sizes
+    uniform in 1..4,096), qProbes per query from {5, 10, 20, 80}, k=20, BF16
+    rerank + FP32 re-score, one graph-replayed persistent launch per batch."""
+    import torch
+    from falconnpp_b200 import synth
+    w = WORKLOADS["mips-1Mx200-L100"]
+    X, _ = make_data(w, 0)
+    Q = synth.mixture(65536, w["d"], n_centres=w["n_centres"], norm_sigma=w["norm_sigma"], seed=3)
+    idx, Xd, _ = _build_index(w, X)
+    rng = np.random.default_rng(11)
+    qps = rng.choice([5, 10, 20, 80], size=len(Q)).astype(np.int32)
+    sizes, s0 = [], 0
+    while s0 < len(Q):
+        b = int(rng.integers(1, 4097))
+        sizes.append((s0, min(len(Q), s0 + b)))
+        s0 += b
+    k = 20
+    Qd = torch.from_numpy(Q).cuda()
+    qpd = torch.from_numpy(qps).cuda()
+    out = torch.zeros((len(Q), k), dtype=torch.int32, device="cuda")
+    stream = torch.cuda.Stream()
+    idx.set_query_form(1, 1, 4)
+    idx.set_option("use_graph", 1)
+
+    def one_pass():
+        for a, b in sizes:
+            idx.query_batched(Qd[a].data_ptr(), b - a, None, qpd[a].data_ptr(), k, 80, out[a].data_ptr(), k,
+                              None, stream.cuda_stream)
+
+    one_pass()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        e0.record()
+        one_pass()
+        e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    ns = 500
+    truth = exact_topk_fp64(Xd, Q[:ns], k)
+    return {"workload": "mixed-1Mx200", "value": round(len(Q) / (ms / 1000.0), 1), "unit": "queries/s",
+            "batches": len(sizes), "ms_total": round(ms, 3), "recall_at_20": round(recall(truth, out[:ns].cpu().numpy(), k), 4),
+            "config": {"queries": len(Q), "batch_sizes": "uniform 1..4096", "qprobes": "per query from {5,10,20,80}",
+                       "k": k, "form": "batched-bf16 x4 shortlist, CUDA graph"}, "data": "synthetic"}
+
+
+def run_serve(args, big=True):
+    """Serving loop (continuous batching) on the 10M x 128 index (or the 1M x 200
+    one): Poisson arrivals at several rates, requests of 1..1,024 queries with
+    k in {1, 10, 100}; p50/p99 request latency, achieved QPS, recall@k on a sample."""
+    import threading
+
+    import torch
+    from falconnpp_b200 import capi, synth
+    if big:
+        w = PRECISION_10M
+        qp = w["qprobes"]
+    else:
+        w = dict(WORKLOADS["mips-1Mx200-L100"], qprobes=10)
+        qp = 10
+    X = synth.mixture(w["n"], w["d"], n_centres=w["n_centres"], norm_sigma=w["norm_sigma"], seed=0)
+    pool = synth.mixture(20000, w["d"], n_centres=w["n_centres"], norm_sigma=w["norm_sigma"], seed=5)
+    idx, Xd, _ = _build_index(w, X)
+    truth = {kk: exact_topk_fp64(Xd, pool[:200], kk) for kk in (1, 10, 100)}
+    idx.set_query_form(1, 1, 4)
+    results = {}
+    for rate in (1000, 10000, 50000, 200000):
+        srv = capi.Server(idx, n_streams=3, memory_budget=256 << 20, max_batch=8192, k_max=100, qprobes_max=qp)
+        rng = np.random.default_rng(rate)
+        duration = 3.0
+        mean_req = 512.5
+        t = 0.0
+        plan = []
+        while t < duration:
+            t += rng.exponential(mean_req / rate)
+            n = int(rng.integers(1, 1025))
+            kk = int(rng.choice([1, 10, 100]))
+            a = int(rng.integers(0, len(pool) - n))
+            plan.append((t, a, n, kk))
+        tickets = []
+        t0 = time.perf_counter()
+        done = []
+
+        def waiter():
+            for tk, (ts, a, n, kk) in tickets_iter():
+                out, lat = srv.wait(tk)
+                done.append((lat, a, n, kk, out))
+
+        q_lock = threading.Condition()
+        pos = [0]
+
+        def tickets_iter():
+            i = 0
+            while i < len(plan):
+                with q_lock:
+                    while i >= len(tickets):
+                        q_lock.wait()
+                    item = tickets[i]
+                yield item
+                i += 1
+
+        th = threading.Thread(target=waiter)
+        th.start()
+        for (ts, a, n, kk) in plan:
+            now = time.perf_counter() - t0
+            if ts > now:
+                time.sleep(ts - now)
+            tk = srv.submit(pool[a:a + n], kk, qp)
+            with q_lock:
+                tickets.append((tk, (ts, a, n, kk)))
+                q_lock.notify()
+        th.join()
+        wall = time.perf_counter() - t0
+        st = srv.stats()
+        srv.close()
+        lats = np.array([d_[0] for d_ in done])
+        nq = sum(d_[2] for d_ in done)
+        rec, cnt = 0.0, 0
+        for lat, a, n, kk, out in done:
+            if a < 200:
+                m = min(n, 200 - a)
+                rec += synth.recall_at_k(truth[kk][a:a + m], out[:m], kk) * m
+                cnt += m
+        results[str(rate)] = {"p50_ms": round(float(np.percentile(lats, 50)), 3),
+                              "p99_ms": round(float(np.percentile(lats, 99)), 3),
+                              "achieved_qps": round(nq / wall, 1), "requests": len(done),
+                              "launches": st["launches"], "recall_sampled": round(rec / cnt, 4) if cnt else None}
+    return {"workload": "serve-10Mx128" if big else "serve-1Mx200", "rates_qps": results, "unit": "ms",
+            "config": {"n": w["n"], "d": w["d"], "request_sizes": "uniform 1..1024", "k": "{1,10,100}",
+                       "qprobes": qp, "streams": 3, "form": "batched-bf16 x4"}, "data": "synthetic"}
+
+
+EXTRA_WORKLOADS = {
+    "precision-10Mx128": run_precision,
+    "mixed-1Mx200": run_mixed,
+    "serve-10Mx128": lambda a: run_serve(a, True),
+    "serve-1Mx200": lambda a: run_serve(a, False),
+}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", default="mips-1Mx200-L100", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="mips-1Mx200-L100", choices=sorted(WORKLOADS) + sorted(EXTRA_WORKLOADS))
     ap.add_argument("--qprobes", type=int, default=0)
     ap.add_argument("--form", default="all", choices=["all"] + FORMS)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
+    if args.workload in EXTRA_WORKLOADS:
+        import torch
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        print(json.dumps(EXTRA_WORKLOADS[args.workload](args)), flush=True)
+        return 0
     w = WORKLOADS[args.workload]
     if args.qprobes:
         w = dict(w, sweep=(args.qprobes,))

@@ -10,7 +10,8 @@
 //     r*k candidates and the top-k of the shortlist; in FP32 mode the kernel
 //     reproduces the plain path bit for bit;
 //   * optional capture of the launch (work-counter reset + kernel) in a CUDA
-//     graph that later calls with the same shape replay.
+//     graph; later calls with the same grid replay it, updating the kernel
+//     node's arguments (batch size, buffers, k, qProbes) in place.
 //
 // Hashing, probe selection and the tie rules are the plain path's
 // (fpp_query.cu): the hash arithmetic stays FP32 and bit-exact.
@@ -99,6 +100,7 @@ fail:
 
 void BatchWorkspace::release() {
   if (graph_exec) cudaGraphExecDestroy(graph_exec);
+  if (graph) cudaGraphDestroy(graph);
   cudaFree(bitset);
   cudaFree(uniq);
   cudaFree(score);
@@ -160,7 +162,8 @@ int batch_query(const Params& P, DeviceIndex& di, BatchWorkspace& bw, const Batc
     return fail(e, "occupancy");
   if (rq.blocks_per_sm > 0) per_sm = std::min(per_sm, rq.blocks_per_sm);
   per_sm = std::max(per_sm, 1);
-  int grid = std::max(1, std::min(rq.nq, nsm * per_sm));
+  // graph mode keeps one grid for every batch size (idle blocks find no work)
+  int grid = std::max(1, rq.use_graph ? nsm * per_sm : std::min(rq.nq, nsm * per_sm));
   const long long nwords = (P.n_points + 31) / 32;
   const long long cap = std::max<long long>(
       1, std::min<long long>(P.n_points, (long long)rq.qprobes_max * std::max<uint32_t>(di.max_kept, 1u)));
@@ -243,7 +246,22 @@ int batch_query(const Params& P, DeviceIndex& di, BatchWorkspace& bw, const Batc
   BatchKey key{rq.Q, rq.nq, rq.q_k, rq.q_qprobes, rq.k_uniform, rq.qprobes_uniform, rq.k_max, rq.qprobes_max,
                rq.shortlist_mult, rq.out,
                rq.out_stride, rq.out_v, rq.mode, grid, kern, bw.bitset, s};
-  if (can_graph && bw.graph_exec && bw.key == key) {
+  // same launch shape (kernel, grid, stream, scratch): the captured graph is
+  // replayed, with the kernel node's arguments updated when they changed
+  const bool same_shape = bw.graph_exec && bw.key.kern == key.kern && bw.key.grid == key.grid &&
+                          bw.key.stream == key.stream && bw.key.bitset == key.bitset;
+  if (can_graph && same_shape) {
+    if (!(bw.key == key)) {
+      cudaKernelNodeParams kp = {};
+      kp.func = const_cast<void*>(kern);
+      kp.gridDim = dim3(grid);
+      kp.blockDim = dim3(kBThreads);
+      kp.sharedMemBytes = (unsigned)ks.smem;
+      kp.kernelParams = args;
+      if ((e = cudaGraphExecKernelNodeSetParams(bw.graph_exec, bw.graph_knode, &kp)) != cudaSuccess)
+        return fail(e, "graph update");
+      bw.key = key;
+    }
     if ((e = cudaGraphLaunch(bw.graph_exec, s)) != cudaSuccess) return fail(e, "graph launch");
     res.graph_replayed = true;
   } else {
@@ -257,9 +275,23 @@ int batch_query(const Params& P, DeviceIndex& di, BatchWorkspace& bw, const Batc
       cudaMemsetAsync(bw.counters, 0, sizeof(unsigned) * 2, s);
       cudaLaunchKernel(kern, dim3(grid), dim3(kBThreads), args, ks.smem, s);
       if ((e = cudaStreamEndCapture(s, &graph)) != cudaSuccess) return fail(e, "capture end");
+      cudaGraphNode_t nodes[4];
+      size_t nn = 4;
+      bw.graph_knode = nullptr;
+      if (cudaGraphGetNodes(graph, nodes, &nn) == cudaSuccess)
+        for (size_t i = 0; i < nn; ++i) {
+          cudaGraphNodeType t;
+          if (cudaGraphNodeGetType(nodes[i], &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) bw.graph_knode = nodes[i];
+        }
       e = cudaGraphInstantiate(&bw.graph_exec, graph, 0);
-      cudaGraphDestroy(graph);
+      if (bw.graph) cudaGraphDestroy(bw.graph);
+      bw.graph = graph;  // kept alive: the kernel node handle belongs to it
       if (e != cudaSuccess) return fail(e, "graph instantiate");
+      if (!bw.graph_knode) {
+        err.code = kErrCuda;
+        err.msg = "batch query: captured graph has no kernel node";
+        return err.code;
+      }
       bw.key = key;
       if ((e = cudaGraphLaunch(bw.graph_exec, s)) != cudaSuccess) return fail(e, "graph launch");
     } else {

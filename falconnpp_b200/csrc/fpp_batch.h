@@ -68,6 +68,8 @@ struct BatchWorkspace {
   int grid = 0;
   unsigned* counters = nullptr;
   cudaGraphExec_t graph_exec = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphNode_t graph_knode = nullptr;
   BatchKey key{};
   void release();
 };
