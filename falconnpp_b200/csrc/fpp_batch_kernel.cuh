@@ -196,7 +196,7 @@ constexpr size_t batch_smem_bytes() {
 __device__ __forceinline__ uint32_t ht_slot(uint32_t id) { return (id * 2654435761u) >> (32 - 13); }
 
 template <int FHT, int MODE, int VI, int VI32>
-__global__ void __launch_bounds__(kBThreads, 3) k_batch_query(BatchArgs a) {
+__global__ void __launch_bounds__(kBThreads, MODE == kRowsF32 ? 2 : 3) k_batch_query(BatchArgs a) {
   constexpr int E = Geo<FHT>::E;
   constexpr int G = Geo<FHT>::G;
   constexpr int WORDS = Geo<FHT>::WORDS;
@@ -247,15 +247,11 @@ __global__ void __launch_bounds__(kBThreads, 3) k_batch_query(BatchArgs a) {
     const int M = L * m;
     const float* qv = a.Q + (size_t)q * a.d;
     for (int i = tid; i < 1024; i += kBThreads) sm.q[i] = i < a.d ? qv[i] : 0.0f;
+    __syncthreads();
 
     // ---- 1. rotate + hash every table (FalconnPP.cpp:358-531)
     {
-      float xr[E];
-#pragma unroll
-      for (int e = 0; e < E; ++e) {
-        const int idx = gl * E + e;
-        xr[e] = idx < a.d ? __ldg(qv + idx) : 0.0f;
-      }
+      const float* xs = sm.q + gl * E;  // the query, zero padded past d
       const int cnt = min(m1 + 1, a.D);
       const int rounds = (L + GROUPS - 1) / GROUPS;
       for (int rd = 0; rd < rounds; ++rd) {
@@ -266,7 +262,7 @@ __global__ void __launch_bounds__(kBThreads, 3) k_batch_query(BatchArgs a) {
         for (int layer = 0; layer < 2; ++layer) {
           float y[E];
 #pragma unroll
-          for (int e = 0; e < E; ++e) y[e] = xr[e];
+          for (int e = 0; e < E; ++e) y[e] = xs[e];
           hd3_rotate<FHT>(y, a.flips + ((size_t)(layer * L + lt) * 3) * WORDS, gl);
           float* lv = sm.gv + (grp * 2 + layer) * (kBMaxM1 + 1);
           int* lc = sm.gc + (grp * 2 + layer) * (kBMaxM1 + 1);
@@ -400,24 +396,30 @@ __global__ void __launch_bounds__(kBThreads, 3) k_batch_query(BatchArgs a) {
         }
         cur = lo;
       }
-      for (uint32_t c0 = c_begin; c0 < c_end; c0 += 128u) {
-        if (!use_bitset && *(volatile unsigned*)&s_ovf) break;
-        uint32_t idv[4];
+      // ids of the next 128-id step are loaded while this step is inserted
+      uint32_t nxt_id[4];
+      auto load_ids = [&](uint32_t c0, uint32_t (&dst)[4]) {
 #pragma unroll
         for (int h = 0; h < 4; ++h) {
           const uint32_t i = c0 + h * 32 + lane;
-          idv[h] = kEmpty;
+          dst[h] = kEmpty;
           if (i < c_end) {
             int p = cur;
             while (s_pe[p] <= i) ++p;
             const uint32_t st = p > 0 ? s_pe[p - 1] : 0u;
-            idv[h] = (uint32_t)__ldg(a.ids + s_po[p] + (i - st));
+            dst[h] = (uint32_t)__ldg(a.ids + s_po[p] + (i - st));
           }
         }
-        {
-          const uint32_t nxt = min(c0 + 128u, c_end - 1);
-          while (cur < Qp - 1 && s_pe[cur] <= nxt) ++cur;
-        }
+        const uint32_t nx = min(c0 + 128u, c_end > 0 ? c_end - 1 : 0u);
+        while (cur < Qp - 1 && s_pe[cur] <= nx) ++cur;
+      };
+      if (c_begin < c_end) load_ids(c_begin, nxt_id);
+      for (uint32_t c0 = c_begin; c0 < c_end; c0 += 128u) {
+        if (!use_bitset && *(volatile unsigned*)&s_ovf) break;
+        uint32_t idv[4];
+#pragma unroll
+        for (int h = 0; h < 4; ++h) idv[h] = nxt_id[h];
+        if (c0 + 128u < c_end) load_ids(c0 + 128u, nxt_id);
         bool fresh[4];
 #pragma unroll
         for (int h = 0; h < 4; ++h) {
@@ -485,7 +487,7 @@ __global__ void __launch_bounds__(kBThreads, 3) k_batch_query(BatchArgs a) {
     __syncthreads();
     {
       const float* scl = MODE == kRowsFP8 ? a.Xscale : nullptr;
-      rerank_rows<MODE, VI, (MODE == kRowsF32 ? 2 : 4)>(uq, U, sc, sm.q, a.Xrows, a.row_bytes, a.nchunk, scl,
+      rerank_rows<MODE, VI, 2>(uq, U, sc, sm.q, a.Xrows, a.row_bytes, a.nchunk, scl,
                                                            warp, kBWarps, lane, s_hist);
     }
     __syncthreads();

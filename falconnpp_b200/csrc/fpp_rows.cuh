@@ -83,7 +83,16 @@ __device__ __forceinline__ void rerank_rows(const uint32_t* ids, unsigned U, uin
   constexpr int EPC = RowFmt<MODE>::EPC;
   const int j = lane & 7;
   const int rsub = lane >> 3;  // which of the warp's 4 rows
-  for (unsigned base = (unsigned)warp * 4 * STEPS; base < U; base += (unsigned)nwarps * 4 * STEPS) {
+  const unsigned stride = (unsigned)nwarps * 4 * STEPS;
+  // the ids of the next step are loaded one step ahead, so a row load never
+  // waits for the id load in front of it
+  uint32_t nid[STEPS];
+#pragma unroll
+  for (int s = 0; s < STEPS; ++s) {
+    const unsigned r = (unsigned)warp * 4 * STEPS + s * 4 + rsub;
+    nid[s] = r < U ? ids[r] : 0u;
+  }
+  for (unsigned base = (unsigned)warp * 4 * STEPS; base < U; base += stride) {
     uint4 data[STEPS][4][VI];
     uint32_t rid[STEPS];
     bool live[STEPS];
@@ -91,7 +100,7 @@ __device__ __forceinline__ void rerank_rows(const uint32_t* ids, unsigned U, uin
     for (int s = 0; s < STEPS; ++s) {
       const unsigned r = base + s * 4 + rsub;
       live[s] = r < U;
-      rid[s] = live[s] ? ids[r] : 0u;
+      rid[s] = nid[s];
       const uint4* row = reinterpret_cast<const uint4*>(rows + (size_t)rid[s] * row_bytes);
 #pragma unroll
       for (int v = 0; v < 4; ++v)
@@ -100,6 +109,11 @@ __device__ __forceinline__ void rerank_rows(const uint32_t* ids, unsigned U, uin
           const int c = j + 8 * v + 32 * i;
           data[s][v][i] = (live[s] && c < nchunk) ? __ldg(row + c) : make_uint4(0u, 0u, 0u, 0u);
         }
+    }
+#pragma unroll
+    for (int s = 0; s < STEPS; ++s) {
+      const unsigned r = base + stride + s * 4 + rsub;
+      nid[s] = r < U ? ids[r] : 0u;
     }
 #pragma unroll
     for (int s = 0; s < STEPS; ++s) {
