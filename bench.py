@@ -147,16 +147,15 @@ def make_data(w, rank):
 
 
 def exact_topk_fp64(X_dev, Q_np, k):
-    """FP64 exact MIPS top-k of a query sample (measurement only)."""
+    """FP64 exact MIPS top-k of a query sample (the library's brute-force kernel)."""
     import torch
-    out = []
-    Xd = X_dev.double()
-    for s in range(0, Q_np.shape[0], 100):
-        q = torch.from_numpy(Q_np[s:s + 100]).cuda().double()
-        sc = q @ Xd.T
-        out.append(torch.topk(sc, k, dim=1).indices.int().cpu().numpy())
-    del Xd
-    return np.concatenate(out)
+    from falconnpp_b200 import capi
+    q = torch.from_numpy(np.ascontiguousarray(Q_np, np.float32)).cuda()
+    out = torch.zeros((Q_np.shape[0], k), dtype=torch.int32, device="cuda")
+    capi.bruteforce_topk_f64(X_dev.data_ptr(), X_dev.shape[0], X_dev.shape[1], q.data_ptr(), Q_np.shape[0], k,
+                             out.data_ptr(), None, torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    return out.cpu().numpy()
 
 
 def recall(truth, ans, k):

@@ -21,6 +21,7 @@ EXPORTED = [
     "fpp_dump_tables", "fpp_build_dump_hash", "fpp_query_dump", "fpp_rerank_probes_noalloc",
     "fpp_set_query_form", "fpp_query_batched", "fpp_autotune",
     "fpp_server_create", "fpp_server_submit", "fpp_server_wait", "fpp_server_stats", "fpp_server_destroy",
+    "fpp_bruteforce_topk_f64",
 ]
 
 _lib = None
@@ -69,6 +70,7 @@ def lib() -> ctypes.CDLL:
             "fpp_server_wait": (i32, [vp, i64, ctypes.POINTER(ctypes.c_double)]),
             "fpp_server_stats": (i32, [vp, vp, i32]),
             "fpp_server_destroy": (None, [vp]),
+            "fpp_bruteforce_topk_f64": (i32, [vp, i64, i32, vp, i32, i32, vp, vp, vp]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -246,3 +248,11 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+def bruteforce_topk_f64(x_ptr: int, n: int, d: int, q_ptr: int, nq: int, k: int, out_ptr: int,
+                        val_ptr: int | None = None, stream: int | None = None) -> None:
+    """Exact FP64 MIPS top-k of device queries against device points (ground truth)."""
+    _check(lib().fpp_bruteforce_topk_f64(ctypes.c_void_p(x_ptr), n, d, ctypes.c_void_p(q_ptr), nq, k,
+                                         ctypes.c_void_p(out_ptr), ctypes.c_void_p(val_ptr or 0),
+                                         ctypes.c_void_p(stream or 0)))

@@ -192,6 +192,17 @@ int fpp_server_wait(fpp_server* s, long long ticket, double* latency_ms);
 int fpp_server_stats(fpp_server* s, double* out, int n);
 void fpp_server_destroy(fpp_server* s);
 
+/* Exact maximum-inner-product top-k in FP64 on the GPU: the ground truth of
+ * recall measurements.  Replaces BF::mips_topK, src/BF.cpp:17-86 (which is
+ * FP32 on the CPU); ties are broken by ascending id.  d_X: n_points x
+ * n_features float32 (the raw or the centred data: the ranking is the same),
+ * d_Q: n_queries x n_features, d_out: n_queries x k int32 ids, d_out_val
+ * (may be NULL): the FP64 inner products.  Independent of any index handle.
+ * Limits: k <= 256, n_features <= 1024.  Returns after the results are
+ * written. */
+int fpp_bruteforce_topk_f64(const float* d_X, long long n_points, int n_features, const float* d_Q, int n_queries,
+                            int k, int32_t* d_out, double* d_out_val, void* stream);
+
 /* No counterpart in the reference.  The gather, deduplicate, rerank and top-k
  * stage of fpp_query for callers that cannot allocate device memory: code
  * recording a CUDA graph, a serving thread that must not stall on cudaMalloc /
