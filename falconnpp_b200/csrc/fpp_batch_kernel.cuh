@@ -139,6 +139,8 @@ __device__ __forceinline__ void block_sort_u64(unsigned long long* a, int n) {
     }
 }
 
+constexpr int kQhStride = 36;  // 32 floats + 4 of padding: segment starts 4 banks apart
+
 // dynamic shared memory of k_batch_query (regions reused phase by phase)
 template <int GROUPS>
 struct BatchSmem {
@@ -152,7 +154,9 @@ struct BatchSmem {
   static constexpr size_t kRhv = kGc + 4 * GROUPS * 2 * (kBMaxM1 + 1);
   static constexpr size_t kRhi = kRhv + 4 * GROUPS * kBMaxM1;
   static constexpr size_t kQ = kRhi + 4 * GROUPS * kBMaxM1;
-  static constexpr size_t kBytes = kQ + 4 * 1024;
+  static constexpr size_t kQx = kQ + 4 * 1024;                  // query parts of the tensor-core rerank
+  static constexpr size_t kQh = kQx + 2048;                     // the query for the rotations, padded
+  static constexpr size_t kBytes = kQh + 4 * kQhStride * 16;
   uint32_t* ht;
   float* lv;
   uint32_t* lb;
@@ -163,6 +167,9 @@ struct BatchSmem {
   float* rhv;
   int* rhi;
   float* q;  // the current query, zero padded to 1024 floats
+  unsigned char* qx;
+  float* qh;  // segment s (32 floats) of the query at qh + s * kQhStride: the
+              // lanes of a rotation group read their segments from distinct banks
   // aliases: gather prefix arrays over the lists; the score histogram over
   // both lists (2048 u32); the probe-cut replay heap in the top region; the
   // re-score arrays and the final replay heap in the hash-set region
@@ -185,7 +192,9 @@ struct BatchSmem {
         gc(reinterpret_cast<int*>(p + kGc)),
         rhv(reinterpret_cast<float*>(p + kRhv)),
         rhi(reinterpret_cast<int*>(p + kRhi)),
-        q(reinterpret_cast<float*>(p + kQ)) {}
+        q(reinterpret_cast<float*>(p + kQ)),
+        qx(p + kQx),
+        qh(reinterpret_cast<float*>(p + kQh)) {}
 };
 
 template <int FHT>
@@ -209,7 +218,7 @@ __global__ void __launch_bounds__(kBThreads, MODE == kRowsF32 ? 2 : 3) k_batch_q
   unsigned long long* s_top = sm.top;
   __shared__ uint32_t hist[256];
   __shared__ uint32_t s_pre, s_rem;
-  __shared__ unsigned s_cnt, s_u, s_sel, s_q, s_ovf, s_bstar, s_above;
+  __shared__ unsigned s_cnt, s_u, s_sel, s_q, s_ovf, s_bstar, s_above, s_qmax;
   __shared__ long long tmp[32];
 
   const int tid = threadIdx.x;
@@ -230,7 +239,10 @@ __global__ void __launch_bounds__(kBThreads, MODE == kRowsF32 ? 2 : 3) k_batch_q
 
   for (;;) {
     __syncthreads();
-    if (tid == 0) s_q = atomicAdd(a.work, 1u);
+    if (tid == 0) {
+      s_q = atomicAdd(a.work, 1u);
+      s_qmax = 0u;
+    }
     __syncthreads();
     const unsigned qu = s_q;
     if (qu >= (unsigned)a.nq) break;
@@ -246,12 +258,25 @@ __global__ void __launch_bounds__(kBThreads, MODE == kRowsF32 ? 2 : 3) k_batch_q
     const int m1 = ceil_sqrt_int(m);     // ceil(sqrt(m)), FalconnPP.cpp:337
     const int M = L * m;
     const float* qv = a.Q + (size_t)q * a.d;
-    for (int i = tid; i < 1024; i += kBThreads) sm.q[i] = i < a.d ? qv[i] : 0.0f;
+    {
+      float amax = 0.0f;  // max |q| (the E4M3 query scale)
+      for (int i = tid; i < 1024; i += kBThreads) {
+        const float x = i < a.d ? qv[i] : 0.0f;
+        sm.q[i] = x;
+        if (i < G * E) sm.qh[(i >> 5) * kQhStride + (i & 31)] = x;
+        amax = fmaxf(amax, fabsf(x));
+      }
+      if (MODE == kRowsFP8) {
+#pragma unroll
+        for (int o = 16; o; o >>= 1) amax = fmaxf(amax, __shfl_xor_sync(kFullMask, amax, o));
+        if (lane == 0) atomicMax(&s_qmax, __float_as_uint(amax));  // non-negative: bits order as values
+      }
+    }
     __syncthreads();
 
     // ---- 1. rotate + hash every table (FalconnPP.cpp:358-531)
     {
-      const float* xs = sm.q + gl * E;  // the query, zero padded past d
+      const float* xs = sm.qh + gl * kQhStride;  // the query segment of this lane, zero padded past d
       const int cnt = min(m1 + 1, a.D);
       const int rounds = (L + GROUPS - 1) / GROUPS;
       for (int rd = 0; rd < rounds; ++rd) {
@@ -365,6 +390,9 @@ __global__ void __launch_bounds__(kBThreads, MODE == kRowsF32 ? 2 : 3) k_batch_q
           const uint32_t g = s_probe[p];
           o = a.bucket_off[g];
           sz = a.bucket_off[g + 1] - o;
+          // the bucket's ids (the 16-byte aligned part, at most 16 KB) into L2
+          const uint32_t w0 = o & ~3u, w1 = min(o + sz, w0 + 4096u) & ~3u;
+          if (w1 > w0) prefetch_l2(a.ids + w0, (w1 - w0) * 4u);
         }
         long long tot;
         const long long ex = block_exclusive_scan((long long)sz, tmp, &tot) + run;
@@ -483,12 +511,20 @@ __global__ void __launch_bounds__(kBThreads, MODE == kRowsF32 ? 2 : 3) k_batch_q
     // ---- 4. rerank the unique rows (FalconnPP.cpp:642-660), with a
     // histogram of the scores' top 11 key bits for the selection below
     uint32_t* s_hist = sm.hist();
+    float qscale = 1.0f;
+    if (MODE == kRowsFP8) {
+      const float qm = __uint_as_float(s_qmax);
+      qscale = qm > 0.0f ? qm / 448.0f : 1.0f;  // 448: largest finite E4M3
+    }
+    if (MODE != kRowsF32) fill_query_parts<MODE>(sm.q, qscale, sm.qx);
     for (int i = tid; i < kHistBins; i += kBThreads) s_hist[i] = 0u;
     __syncthreads();
-    {
-      const float* scl = MODE == kRowsFP8 ? a.Xscale : nullptr;
-      rerank_rows<MODE, VI, 2>(uq, U, sc, sm.q, a.Xrows, a.row_bytes, a.nchunk, scl,
-                                                           warp, kBWarps, lane, s_hist);
+    if (MODE == kRowsF32) {
+      rerank_rows<MODE, VI, 2>(uq, U, sc, sm.q, a.Xrows, a.row_bytes, a.nchunk, nullptr, warp, kBWarps, lane,
+                               s_hist);
+    } else {
+      rerank_rows_mma<MODE>(uq, U, sc, sm.qx, a.Xrows, a.row_bytes, a.nchunk, a.Xscale, qscale, warp, kBWarps,
+                            lane, s_hist);
     }
     __syncthreads();
 
@@ -667,8 +703,8 @@ static KernelSel pick_fht(int fht) {
   }
 }
 
-// per-precision selection (VI: 16-byte chunks per virtual lane of the first
-// rerank; VI32: of the FP32 rows), defined in fpp_batch_{f32,bf16,fp8}.cu
+// per-precision selection (VI: 16-byte chunks per virtual lane of the FP32
+// first rerank; VI32: of the FP32 re-score), defined in fpp_batch_{f32,bf16,fp8}.cu
 KernelSel pick_kernel_f32(int fht, int d);
 KernelSel pick_kernel_bf16(int fht, int d);
 KernelSel pick_kernel_fp8(int fht, int d);

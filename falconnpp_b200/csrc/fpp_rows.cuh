@@ -21,6 +21,7 @@
 namespace fpp {
 
 enum RowMode : int { kRowsF32 = 0, kRowsBF16 = 1, kRowsFP8 = 2 };
+constexpr uint32_t kNoRow = 0xffffffffu;
 
 template <int MODE>
 struct RowFmt {
@@ -58,6 +59,12 @@ __device__ __forceinline__ void unpack_chunk_fp8(const uint4& u, float* x) {
   }
 }
 
+// bulk prefetch of `bytes` (a multiple of 16) at a 16-byte aligned global
+// address into L2; no registers or shared memory are held while it is in flight
+__device__ __forceinline__ void prefetch_l2(const void* p, uint32_t bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(p), "r"(bytes));
+}
+
 template <int MODE>
 __device__ __forceinline__ void unpack_chunk(const uint4& u, float* x) {
   if (MODE == kRowsF32)
@@ -92,7 +99,23 @@ __device__ __forceinline__ void rerank_rows(const uint32_t* ids, unsigned U, uin
     const unsigned r = (unsigned)warp * 4 * STEPS + s * 4 + rsub;
     nid[s] = r < U ? ids[r] : 0u;
   }
+  // rows of the step after next are prefetched into L2 (lane i < 4 * STEPS
+  // takes row i of that step); their ids are loaded one step before that
+  const bool pf_lane = lane < 4 * STEPS;
+  const uint32_t pf_bytes = (uint32_t)row_bytes;
+  uint32_t pf_id = kNoRow;
+  if (pf_lane) {
+    const unsigned r = (unsigned)warp * 4 * STEPS + stride + lane;
+    if (r < U) prefetch_l2(rows + (size_t)ids[r] * row_bytes, pf_bytes);
+    const unsigned r2 = r + stride;
+    pf_id = r2 < U ? ids[r2] : kNoRow;
+  }
   for (unsigned base = (unsigned)warp * 4 * STEPS; base < U; base += stride) {
+    if (pf_id != kNoRow) prefetch_l2(rows + (size_t)pf_id * row_bytes, pf_bytes);
+    if (pf_lane) {
+      const unsigned r3 = base + 3 * stride + lane;
+      pf_id = r3 < U ? ids[r3] : kNoRow;
+    }
     uint4 data[STEPS][4][VI];
     uint32_t rid[STEPS];
     bool live[STEPS];
@@ -147,6 +170,169 @@ __device__ __forceinline__ void rerank_rows(const uint32_t* ids, unsigned U, uin
       if (MODE == kRowsFP8) t = __fmul_rn(t, live[s] ? __ldg(scale + rid[s]) : 0.0f);
       if (j == 0 && live[s]) {
         score[base + s * 4 + rsub] = __float_as_uint(t);
+        if (hist11) atomicAdd(hist11 + (ord_key_bits(__float_as_uint(t)) >> 21), 1u);
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Tensor-core rerank of BF16 / FP8-E4M3 rows (the approximate first pass of
+// the batched form; its scores only pick the shortlist that is re-scored in
+// FP32 with the parity order above).
+//
+// A warp takes 16 rows at a time and computes D[16 x 8] = rows[16 x K] *
+// B[K x 8] with mma.sync (m16n8k16 BF16 or m16n8k32 E4M3, FP32 accumulate).
+// Column n of B holds part n of the query: BF16 hi and lo (q ~ hi + lo to 16
+// mantissa bits), or three E4M3 terms of q / qscale; the other columns are 0,
+// so the score of a row is the sum of its 8 accumulator columns.
+//
+// Lane (g, c) = (lane / 4, lane % 4) loads 16-byte chunk 4j + c of rows g and
+// g + 8; the 16 bytes are its A registers for two k-steps.  The k positions
+// of a fragment are a permutation of the dimensions, the same for A and B
+// (B column g is loaded by lanes with group g from the same chunk of the
+// query part), so the products pair row and query elements of the same
+// dimension.  Loads are issued four chunks (eight 16-byte loads per lane) at
+// a time; the ids of the warp's next tile are loaded one tile ahead.
+__device__ __forceinline__ void mma_bf16_m16n8k16(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
+                                                  uint32_t b0, uint32_t b1) {
+  asm("mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+__device__ __forceinline__ void mma_e4m3_m16n8k32(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
+                                                  uint32_t b0, uint32_t b1) {
+  asm("mma.sync.aligned.m16n8k32.row.col.f32.e4m3.e4m3.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+template <int MODE>
+struct QueryParts {
+  static constexpr int NP = MODE == kRowsBF16 ? 2 : 3;   // B columns in use
+  static constexpr int PC = MODE == kRowsBF16 ? 64 : 32; // 16-byte chunks per part (d <= 512)
+  static constexpr int EPC = RowFmt<MODE>::EPC;
+  static constexpr int kBytes = NP * PC * 16;
+};
+
+// the query parts of the tensor-core rerank, from the FP32 query qs (zero
+// padded to 1024): BF16 hi = bf16(q), lo = bf16(q - hi); E4M3 terms of
+// y = q / qscale: h = e4m3(y), m = e4m3(y - h), l = e4m3(y - h - m).  Called
+// by all threads of the block; the caller synchronises before use.
+template <int MODE>
+__device__ __forceinline__ void fill_query_parts(const float* qs, float qscale, unsigned char* qx) {
+  using P = QueryParts<MODE>;
+  constexpr int per_part = P::PC * P::EPC;
+  for (int e = threadIdx.x; e < per_part; e += blockDim.x) {
+    const float x = qs[e];
+    if (MODE == kRowsBF16) {
+      const __nv_bfloat16 hi = __float2bfloat16_rn(x);
+      const __nv_bfloat16 lo = __float2bfloat16_rn(x - __bfloat162float(hi));
+      reinterpret_cast<__nv_bfloat16*>(qx)[e] = hi;
+      reinterpret_cast<__nv_bfloat16*>(qx)[per_part + e] = lo;
+    } else {
+      float y = x / qscale;
+#pragma unroll
+      for (int p = 0; p < P::NP; ++p) {
+        const __nv_fp8_storage_t t = __nv_cvt_float_to_fp8(y, __NV_SATFINITE, __NV_E4M3);
+        qx[p * per_part + e] = (unsigned char)t;
+        const __half_raw hr = __nv_cvt_fp8_to_halfraw(t, __NV_E4M3);
+        y = y - __half2float(*reinterpret_cast<const __half*>(&hr));
+      }
+    }
+  }
+}
+
+template <int MODE>
+__device__ __forceinline__ void rerank_rows_mma(const uint32_t* ids, unsigned U, uint32_t* score,
+                                                const unsigned char* qx, const unsigned char* rows, size_t row_bytes,
+                                                int nchunk, const float* scale, float qscale, int warp, int nwarps,
+                                                int lane, uint32_t* hist11) {
+  using P = QueryParts<MODE>;
+  const int g = lane >> 2;
+  const int c = lane & 3;
+  const int JN = (nchunk + 3) >> 2;
+  const unsigned ntiles = (U + 15u) >> 4;
+  const uint4* qpart = reinterpret_cast<const uint4*>(qx) + (g < P::NP ? g : 0) * P::PC + c;
+  const uint4 zero = make_uint4(0u, 0u, 0u, 0u);
+  unsigned tile = (unsigned)warp;
+  const unsigned nw = (unsigned)nwarps;
+  uint32_t nid0 = 0u, nid1 = 0u;
+  if (tile < ntiles) {
+    const unsigned r0 = tile * 16u + g;
+    nid0 = r0 < U ? ids[r0] : 0u;
+    nid1 = r0 + 8u < U ? ids[r0 + 8u] : 0u;
+  }
+  // the rows of the warp's next two tiles are prefetched into L2: lane 2i + h
+  // (i < 8, h < 2) takes row i + 8h; the ids of a tile are loaded one tile
+  // before its prefetch is issued
+  const bool pf_lane = lane < 16;
+  const unsigned pf_row = (unsigned)(lane >> 1) + 8u * (unsigned)(lane & 1);
+  const uint32_t pf_bytes = (uint32_t)row_bytes;
+  uint32_t pf_id = kNoRow;
+  if (pf_lane) {
+    const unsigned r = (tile + nw) * 16u + pf_row;
+    if (r < U) prefetch_l2(rows + (size_t)ids[r] * row_bytes, pf_bytes);
+    const unsigned r2 = (tile + 2u * nw) * 16u + pf_row;
+    pf_id = r2 < U ? ids[r2] : kNoRow;
+  }
+  for (; tile < ntiles; tile += nw) {
+    if (pf_id != kNoRow) prefetch_l2(rows + (size_t)pf_id * row_bytes, pf_bytes);
+    if (pf_lane) {
+      const unsigned r3 = (tile + 3u * nw) * 16u + pf_row;
+      pf_id = r3 < U ? ids[r3] : kNoRow;
+    }
+    const unsigned r0 = tile * 16u + g;
+    const unsigned r1 = r0 + 8u;
+    const bool l0 = r0 < U, l1 = r1 < U;
+    const uint32_t id0 = nid0, id1 = nid1;
+    {
+      const unsigned n0 = r0 + 16u * (unsigned)nwarps;
+      nid0 = n0 < U ? ids[n0] : 0u;
+      nid1 = n0 + 8u < U ? ids[n0 + 8u] : 0u;
+    }
+    const uint4* p0 = reinterpret_cast<const uint4*>(rows + (size_t)id0 * row_bytes) + c;
+    const uint4* p1 = reinterpret_cast<const uint4*>(rows + (size_t)id1 * row_bytes) + c;
+    float acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    for (int j0 = 0; j0 < JN; j0 += 4) {
+      uint4 x0[4], x1[4];
+#pragma unroll
+      for (int jj = 0; jj < 4; ++jj) {
+        const bool ok = 4 * (j0 + jj) + c < nchunk;
+        x0[jj] = (ok && l0) ? __ldg(p0 + 4 * (j0 + jj)) : zero;
+        x1[jj] = (ok && l1) ? __ldg(p1 + 4 * (j0 + jj)) : zero;
+      }
+#pragma unroll
+      for (int jj = 0; jj < 4; ++jj) {
+        if (j0 + jj < JN) {
+          const uint4 b = g < P::NP ? qpart[4 * (j0 + jj)] : zero;
+          if (MODE == kRowsBF16) {
+            mma_bf16_m16n8k16(acc, x0[jj].x, x1[jj].x, x0[jj].y, x1[jj].y, b.x, b.y);
+            mma_bf16_m16n8k16(acc, x0[jj].z, x1[jj].z, x0[jj].w, x1[jj].w, b.z, b.w);
+          } else {
+            mma_e4m3_m16n8k32(acc, x0[jj].x, x1[jj].x, x0[jj].y, x1[jj].y, b.x, b.y);
+            mma_e4m3_m16n8k32(acc, x0[jj].z, x1[jj].z, x0[jj].w, x1[jj].w, b.z, b.w);
+          }
+        }
+      }
+    }
+    // row g: columns 2c, 2c+1 in acc[0..1]; row g + 8 in acc[2..3]
+    float s0 = acc[0] + acc[1];
+    float s1 = acc[2] + acc[3];
+    s0 += __shfl_xor_sync(0xffffffffu, s0, 1);
+    s1 += __shfl_xor_sync(0xffffffffu, s1, 1);
+    s0 += __shfl_xor_sync(0xffffffffu, s0, 2);
+    s1 += __shfl_xor_sync(0xffffffffu, s1, 2);
+    if (c == 0) {
+      if (l0) {
+        const float t = MODE == kRowsFP8 ? s0 * qscale * __ldg(scale + id0) : s0;
+        score[r0] = __float_as_uint(t);
+        if (hist11) atomicAdd(hist11 + (ord_key_bits(__float_as_uint(t)) >> 21), 1u);
+      }
+      if (l1) {
+        const float t = MODE == kRowsFP8 ? s1 * qscale * __ldg(scale + id1) : s1;
+        score[r1] = __float_as_uint(t);
         if (hist11) atomicAdd(hist11 + (ord_key_bits(__float_as_uint(t)) >> 21), 1u);
       }
     }
