@@ -22,7 +22,10 @@ constexpr int kBMaxProbes = 1024;
 constexpr int kBMaxM1 = 16;
 constexpr int kBMaxTop = 1024;    // k * shortlist multiple, and the replay heaps
 constexpr int kHT = 8192;         // shared-memory hash set for the dedupe (2^13 slots)
-constexpr unsigned kHTLimit = kHT - 2048;  // unique ids before switching to the L2 bitset
+constexpr int kGPerLane = 8;      // candidate ids per lane per gather step
+constexpr uint32_t kGStep = 32 * kGPerLane;
+constexpr unsigned kHTLimit = 5120;  // unique ids before switching to the L2 bitset
+static_assert(kHTLimit - 1 + kBWarps * kGStep < (unsigned)kHT, "the hash set must keep an empty slot");
 constexpr uint32_t kEmpty = 0xffffffffu;
 constexpr int kHistBins = 2048;   // top 11 bits of the score key
 
@@ -412,7 +415,7 @@ __global__ void __launch_bounds__(kBThreads, MODE == kRowsF32 ? 2 : 3) k_batch_q
     const unsigned cap = (unsigned)a.cap;
     bool use_bitset = false;
     for (int pass = 0; pass < 2; ++pass) {
-      const uint32_t per = (((C + kBWarps - 1) / kBWarps) + 127u) & ~127u;
+      const uint32_t per = (((C + kBWarps - 1) / kBWarps) + (kGStep - 1)) & ~(kGStep - 1);
       const uint32_t c_begin = min(C, (uint32_t)warp * per);
       const uint32_t c_end = min(C, c_begin + per);
       int cur = 0;
@@ -424,64 +427,76 @@ __global__ void __launch_bounds__(kBThreads, MODE == kRowsF32 ? 2 : 3) k_batch_q
         }
         cur = lo;
       }
-      // ids of the next 128-id step are loaded while this step is inserted
-      uint32_t nxt_id[4];
-      auto load_ids = [&](uint32_t c0, uint32_t (&dst)[4]) {
+      // ids of the next step are loaded while this step is inserted
+      uint32_t nxt_id[kGPerLane];
+      auto load_ids = [&](uint32_t c0, uint32_t (&dst)[kGPerLane]) {
+        int p = cur;  // probes rise with h
 #pragma unroll
-        for (int h = 0; h < 4; ++h) {
+        for (int h = 0; h < kGPerLane; ++h) {
           const uint32_t i = c0 + h * 32 + lane;
           dst[h] = kEmpty;
           if (i < c_end) {
-            int p = cur;
             while (s_pe[p] <= i) ++p;
             const uint32_t st = p > 0 ? s_pe[p - 1] : 0u;
             dst[h] = (uint32_t)__ldg(a.ids + s_po[p] + (i - st));
           }
         }
-        const uint32_t nx = min(c0 + 128u, c_end > 0 ? c_end - 1 : 0u);
+        const uint32_t nx = min(c0 + kGStep, c_end > 0 ? c_end - 1 : 0u);
         while (cur < Qp - 1 && s_pe[cur] <= nx) ++cur;
       };
       if (c_begin < c_end) load_ids(c_begin, nxt_id);
-      for (uint32_t c0 = c_begin; c0 < c_end; c0 += 128u) {
+      for (uint32_t c0 = c_begin; c0 < c_end; c0 += kGStep) {
         if (!use_bitset && *(volatile unsigned*)&s_ovf) break;
-        uint32_t idv[4];
+        uint32_t idv[kGPerLane];
 #pragma unroll
-        for (int h = 0; h < 4; ++h) idv[h] = nxt_id[h];
-        if (c0 + 128u < c_end) load_ids(c0 + 128u, nxt_id);
-        bool fresh[4];
+        for (int h = 0; h < kGPerLane; ++h) idv[h] = nxt_id[h];
+        if (c0 + kGStep < c_end) load_ids(c0 + kGStep, nxt_id);
+        bool fresh[kGPerLane];
+        if (use_bitset) {
 #pragma unroll
-        for (int h = 0; h < 4; ++h) {
-          fresh[h] = false;
-          const uint32_t id = idv[h];
-          if (id != kEmpty) {
-            if (use_bitset) {
-              const uint32_t bit = 1u << (id & 31u);
-              fresh[h] = (atomicOr(bits + (id >> 5), bit) & bit) == 0u;
-            } else {
-              // linear probing; the table never holds more than kHTLimit +
-              // 1024 ids, so an empty slot always exists
-              uint32_t slot = ht_slot(id);
-              for (;;) {
-                const uint32_t old = atomicCAS(sm.ht + slot, kEmpty, id);
-                if (old == kEmpty) {
-                  fresh[h] = true;
-                  break;
-                }
-                if (old == id) break;
-                slot = (slot + 1) & (kHT - 1);
-              }
+          for (int h = 0; h < kGPerLane; ++h) {
+            const uint32_t id = idv[h];
+            const uint32_t bit = 1u << (id & 31u);
+            fresh[h] = id != kEmpty && (atomicOr(bits + (id >> 5), bit) & bit) == 0u;
+          }
+        } else {
+          // linear probing: every first probe is issued before any collision
+          // is followed.  At most kHTLimit - 1 + kBWarps * kGStep ids are ever
+          // in the table (each warp finishes at most one step after the count
+          // reaches the limit), so an empty slot always exists.
+          uint32_t slot[kGPerLane], old[kGPerLane];
+#pragma unroll
+          for (int h = 0; h < kGPerLane; ++h) {
+            slot[h] = ht_slot(idv[h]);
+            old[h] = idv[h] != kEmpty ? atomicCAS(sm.ht + slot[h], kEmpty, idv[h]) : kEmpty;  // no id: done
+          }
+#pragma unroll
+          for (int h = 0; h < kGPerLane; ++h) {
+            while (old[h] != kEmpty && old[h] != idv[h]) {
+              slot[h] = (slot[h] + 1) & (kHT - 1);
+              old[h] = atomicCAS(sm.ht + slot[h], kEmpty, idv[h]);
             }
+            fresh[h] = idv[h] != kEmpty && old[h] == kEmpty;
           }
         }
+        // one position reservation per warp step
+        unsigned bal[kGPerLane];
+        unsigned nfresh = 0;
 #pragma unroll
-        for (int h = 0; h < 4; ++h) {
-          const unsigned bal = __ballot_sync(kFullMask, fresh[h]);
-          if (bal) {
-            unsigned base = 0;
-            if (lane == 0) base = atomicAdd(&s_u, (unsigned)__popc(bal));
-            base = __shfl_sync(kFullMask, base, 0);
-            const unsigned pos = base + __popc(bal & ((1u << lane) - 1u));
+        for (int h = 0; h < kGPerLane; ++h) {
+          bal[h] = __ballot_sync(kFullMask, fresh[h]);
+          nfresh += __popc(bal[h]);
+        }
+        if (nfresh) {
+          unsigned base = 0;
+          if (lane == 0) base = atomicAdd(&s_u, nfresh);
+          base = __shfl_sync(kFullMask, base, 0);
+          const unsigned below = (1u << lane) - 1u;
+#pragma unroll
+          for (int h = 0; h < kGPerLane; ++h) {
+            const unsigned pos = base + __popc(bal[h] & below);
             if (fresh[h] && pos < cap) uq[pos] = idv[h];
+            base += __popc(bal[h]);
           }
         }
         if (!use_bitset && lane == 0 && *(volatile unsigned*)&s_u >= kHTLimit) s_ovf = 1u;
