@@ -114,6 +114,39 @@ __device__ __forceinline__ uint32_t block_select(int n, unsigned want, F key_at,
   return t;
 }
 
+// The bin of a kHistBins-bin histogram (counts by key bits, larger bin =
+// larger keys) that holds the want-th largest key, for 1 <= want <= total:
+// *bin, *above = the count in bins >= it, *inbin = the count in it.  Thread t
+// owns bins [kHistBins - 8(t+1), kHistBins - 8t), scanned from the top; needs
+// blockDim.x * 8 == kHistBins.  Ends with a barrier.
+__device__ __forceinline__ void hist_find(const uint32_t* h, unsigned want, long long* tmp, unsigned* bin,
+                                          unsigned* above_out, unsigned* inbin) {
+  const int tid = threadIdx.x;
+  uint32_t c[8];
+  uint32_t sum = 0;
+  const int hi = kHistBins - 8 * tid;
+#pragma unroll
+  for (int b = 0; b < 8; ++b) {
+    c[b] = h[hi - 1 - b];
+    sum += c[b];
+  }
+  long long tot;
+  const long long above = block_exclusive_scan((long long)sum, tmp, &tot);
+  if (above < (long long)want && above + sum >= want) {
+    long long cum = above;
+#pragma unroll
+    for (int b = 0; b < 8; ++b) {
+      if (cum + c[b] >= want && cum < (long long)want) {
+        *bin = (unsigned)(hi - 1 - b);
+        *above_out = (unsigned)(cum + c[b]);
+        *inbin = c[b];
+      }
+      cum += c[b];
+    }
+  }
+  __syncthreads();
+}
+
 // ascending bitonic sort of n (<= kBMaxTop) 64-bit keys in shared memory
 __device__ __forceinline__ void block_sort_u64(unsigned long long* a, int n) {
   int N = 1;
@@ -221,7 +254,7 @@ __global__ void __launch_bounds__(kBThreads, MODE == kRowsF32 ? 2 : 3) k_batch_q
   unsigned long long* s_top = sm.top;
   __shared__ uint32_t hist[256];
   __shared__ uint32_t s_pre, s_rem;
-  __shared__ unsigned s_cnt, s_u, s_sel, s_q, s_ovf, s_bstar, s_above, s_qmax;
+  __shared__ unsigned s_cnt, s_u, s_sel, s_q, s_ovf, s_bstar, s_above, s_inbin, s_qmax;
   __shared__ long long tmp[32];
 
   const int tid = threadIdx.x;
@@ -282,7 +315,10 @@ __global__ void __launch_bounds__(kBThreads, MODE == kRowsF32 ? 2 : 3) k_batch_q
       const float* xs = sm.qh + gl * kQhStride;  // the query segment of this lane, zero padded past d
       const int cnt = min(m1 + 1, a.D);
       const int rounds = (L + GROUPS - 1) / GROUPS;
+      constexpr int kGroupsPerWarp = 32 / G;
       for (int rd = 0; rd < rounds; ++rd) {
+        // a warp whose groups all have no table left stops (warp-uniform)
+        if (rd * GROUPS + warp * kGroupsPerWarp >= L) break;
         const int l = rd * GROUPS + grp;
         const bool active = l < L;
         const int lt = active ? l : 0;
@@ -548,89 +584,72 @@ __global__ void __launch_bounds__(kBThreads, MODE == kRowsF32 ? 2 : 3) k_batch_q
     const unsigned R = MODE == kRowsF32 ? kk : min((unsigned)kBMaxTop, kk * (unsigned)a.shortlist_mult);
     unsigned nsel = U;
     bool exact = true;
+    uint32_t* sid = sm.sid();
+    uint32_t* ssc = sm.ssc();
+    // the shortlist (ids and first scores) goes to sid/ssc: every candidate
+    // whose key reaches the cut t, which is the bin of the R-th largest key
+    // (refined by the next 11 key bits when that bin holds many)
     if (U > R) {
-      // the bin holding the R-th largest key: thread t owns bins
-      // [2048 - 8(t+1), 2048 - 8t), scanned from the top
-      {
-        uint32_t c[8];
-        uint32_t sum = 0;
-        const int hi = kHistBins - 8 * tid;
-#pragma unroll
-        for (int b = 0; b < 8; ++b) {
-          c[b] = s_hist[hi - 1 - b];
-          sum += c[b];
-        }
-        long long tot;
-        const long long above = block_exclusive_scan((long long)sum, tmp, &tot);
-        if (above < (long long)R && above + sum >= R) {
-          long long cum = above;
-#pragma unroll
-          for (int b = 0; b < 8; ++b) {
-            if (cum + c[b] >= R && cum < (long long)R) {
-              s_bstar = (uint32_t)(hi - 1 - b);
-              s_above = (uint32_t)(cum + c[b]);
-            }
-            cum += c[b];
+      hist_find(s_hist, R, tmp, &s_bstar, &s_above, &s_inbin);
+      const uint32_t bstar = s_bstar;
+      const unsigned above = s_above, inbin = s_inbin;
+      bool take = true;
+      uint32_t t = bstar << 21;
+      if (above <= (unsigned)kBMaxTop) {
+        if (above > R + R / 2 + 32) {
+          for (int i = tid; i < kHistBins; i += kBThreads) s_hist[i] = 0u;
+          __syncthreads();
+          for (unsigned i = tid; i < U; i += kBThreads) {
+            const uint32_t key = ord_key_bits(sc[i]);
+            if ((key >> 21) == bstar) atomicAdd(s_hist + ((key >> 10) & (kHistBins - 1)), 1u);
           }
+          __syncthreads();
+          hist_find(s_hist, R - (above - inbin), tmp, &s_bstar, &s_above, &s_inbin);
+          t |= s_bstar << 10;
+        }
+      } else {
+        // very many equal top bits: radix selection of the R-th key
+        unsigned ge;
+        t = block_select((int)U, R, [&](int i) { return ord_key_bits(sc[i]); }, hist, &s_pre, &s_rem, &s_cnt, &ge);
+        if (MODE == kRowsF32 && ge != R) {
+          exact = false;
+          take = false;
         }
       }
-      __syncthreads();
-      const uint32_t bstar = s_bstar;
-      if (s_above <= (unsigned)kBMaxTop) {
+      if (take) {
         if (tid == 0) s_sel = 0;
         __syncthreads();
         for (unsigned i = tid; i < U; i += kBThreads) {
           const uint32_t key = ord_key_bits(sc[i]);
-          if ((key >> 21) >= bstar) {
+          if (key >= t) {
             const unsigned pos = atomicAdd(&s_sel, 1u);
-            s_top[pos] = ((unsigned long long)(~key) << 32) | uq[i];
+            if (pos < (unsigned)kBMaxTop) {
+              sid[pos] = uq[i];
+              ssc[pos] = sc[i];
+            }
           }
         }
         __syncthreads();
-        nsel = s_sel;
-      } else {
-        // very many equal top bits: radix selection of the R-th key
-        unsigned ge;
-        const uint32_t t = block_select((int)U, R, [&](int i) { return ord_key_bits(sc[i]); }, hist, &s_pre,
-                                        &s_rem, &s_cnt, &ge);
-        if (MODE == kRowsF32 && ge != R) {
-          exact = false;
-        } else {
-          if (tid == 0) s_sel = 0;
-          __syncthreads();
-          for (unsigned i = tid; i < U; i += kBThreads) {
-            const uint32_t key = ord_key_bits(sc[i]);
-            if (key >= t) {
-              const unsigned pos = atomicAdd(&s_sel, 1u);
-              if (pos < (unsigned)kBMaxTop) s_top[pos] = ((unsigned long long)(~key) << 32) | uq[i];
-            }
-          }
-          __syncthreads();
-          nsel = min(s_sel, (unsigned)kBMaxTop);
-        }
+        nsel = min(s_sel, (unsigned)kBMaxTop);
       }
     } else {
-      for (unsigned i = tid; i < U; i += kBThreads)
-        s_top[i] = ((unsigned long long)(~ord_key_bits(sc[i])) << 32) | uq[i];
+      for (unsigned i = tid; i < U; i += kBThreads) {
+        sid[i] = uq[i];
+        ssc[i] = sc[i];
+      }
       __syncthreads();
     }
     if (exact) {
-      block_sort_u64(s_top, (int)nsel);
       if (MODE != kRowsF32) {
-        // exact FP32 re-score of the best R with the parity dot order
-        nsel = min(nsel, R);
-        uint32_t* sid = sm.sid();
-        uint32_t* ssc = sm.ssc();
-        for (unsigned i = tid; i < nsel; i += kBThreads) sid[i] = (uint32_t)s_top[i];
-        __syncthreads();
+        // exact FP32 re-score of the shortlist with the parity dot order
         rerank_rows<kRowsF32, VI32>(sid, nsel, ssc, sm.q, reinterpret_cast<const unsigned char*>(a.Xc),
                                     (size_t)a.ld * 4, a.ld / 4, nullptr, warp, kBWarps, lane, nullptr);
         __syncthreads();
-        for (unsigned i = tid; i < nsel; i += kBThreads)
-          s_top[i] = ((unsigned long long)(~ord_key_bits(ssc[i])) << 32) | sid[i];
-        __syncthreads();
-        block_sort_u64(s_top, (int)nsel);
       }
+      for (unsigned i = tid; i < nsel; i += kBThreads)
+        s_top[i] = ((unsigned long long)(~ord_key_bits(ssc[i])) << 32) | sid[i];
+      __syncthreads();
+      block_sort_u64(s_top, (int)nsel);
       const unsigned kept = min(nsel, kk);
       unsigned dup = 0;
       // equal FP32 scores in the kept list, or at the k-th place: heap order decides
