@@ -264,10 +264,12 @@ __device__ __forceinline__ void rerank_rows_mma(const uint32_t* ids, unsigned U,
     nid0 = r0 < U ? ids[r0] : 0u;
     nid1 = r0 + 8u < U ? ids[r0 + 8u] : 0u;
   }
-  // the rows of the warp's next two tiles are prefetched into L2: lane 2i + h
-  // (i < 8, h < 2) takes row i + 8h; the ids of a tile are loaded one tile
-  // before its prefetch is issued
-  const bool pf_lane = lane < 16;
+  // when a tile takes more than one round of loads (rows longer than 256
+  // bytes), the rows of the warp's next two tiles are prefetched into L2:
+  // lane 2i + h (i < 8, h < 2) takes row i + 8h; the ids of a tile are loaded
+  // one tile before its prefetch is issued.  With one round per tile the
+  // prefetch costs more than it hides.
+  const bool pf_lane = lane < 16 && JN > 4;
   const unsigned pf_row = (unsigned)(lane >> 1) + 8u * (unsigned)(lane & 1);
   const uint32_t pf_bytes = (uint32_t)row_bytes;
   uint32_t pf_id = kNoRow;
@@ -291,6 +293,12 @@ __device__ __forceinline__ void rerank_rows_mma(const uint32_t* ids, unsigned U,
       const unsigned n0 = r0 + 16u * (unsigned)nwarps;
       nid0 = n0 < U ? ids[n0] : 0u;
       nid1 = n0 + 8u < U ? ids[n0 + 8u] : 0u;
+    }
+    // the FP8 row scales are loaded together with the rows
+    float f0 = 1.0f, f1 = 1.0f;
+    if (MODE == kRowsFP8 && c == 0) {
+      f0 = l0 ? __ldg(scale + id0) : 0.0f;
+      f1 = l1 ? __ldg(scale + id1) : 0.0f;
     }
     const uint4* p0 = reinterpret_cast<const uint4*>(rows + (size_t)id0 * row_bytes) + c;
     const uint4* p1 = reinterpret_cast<const uint4*>(rows + (size_t)id1 * row_bytes) + c;
@@ -326,12 +334,12 @@ __device__ __forceinline__ void rerank_rows_mma(const uint32_t* ids, unsigned U,
     s1 += __shfl_xor_sync(0xffffffffu, s1, 2);
     if (c == 0) {
       if (l0) {
-        const float t = MODE == kRowsFP8 ? s0 * qscale * __ldg(scale + id0) : s0;
+        const float t = MODE == kRowsFP8 ? s0 * qscale * f0 : s0;
         score[r0] = __float_as_uint(t);
         if (hist11) atomicAdd(hist11 + (ord_key_bits(__float_as_uint(t)) >> 21), 1u);
       }
       if (l1) {
-        const float t = MODE == kRowsFP8 ? s1 * qscale * __ldg(scale + id1) : s1;
+        const float t = MODE == kRowsFP8 ? s1 * qscale * f1 : s1;
         score[r1] = __float_as_uint(t);
         if (hist11) atomicAdd(hist11 + (ord_key_bits(__float_as_uint(t)) >> 21), 1u);
       }
