@@ -59,6 +59,68 @@ __global__ void k_rows_fp8(const float* __restrict__ Xc, long long n, int ld, in
   }
 }
 
+// ---------------------------------------------------------------- query order
+// A batch is processed grouped by each query's best bucket code in layer 0 of
+// table 0 (the cross-polytope code of its largest rotated coordinate): the
+// queries in flight at the same time then probe overlapping buckets and rows,
+// which stay in L2.  Each query is computed independently, so the order
+// changes no result.
+constexpr int kOrderMaxBins = 1024;  // 2 * n_proj codes
+
+template <int FHT>
+__global__ void __launch_bounds__(256) k_order_key(const float* __restrict__ Q, int nq, int d,
+                                                   const uint32_t* __restrict__ flips, int D, int log2D,
+                                                   uint32_t* __restrict__ key, uint32_t* __restrict__ hist) {
+  constexpr int E = Geo<FHT>::E;
+  constexpr int G = Geo<FHT>::G;
+  const int gl = threadIdx.x & (G - 1);
+  const long long q = (long long)blockIdx.x * (blockDim.x / G) + threadIdx.x / G;
+  const bool active = q < nq;  // inactive groups still join every shuffle
+  float y[E];
+#pragma unroll
+  for (int e = 0; e < E; ++e) {
+    const int idx = gl * E + e;
+    y[e] = (active && idx < d) ? __ldg(Q + (size_t)q * d + idx) : 0.0f;
+  }
+  hd3_rotate<FHT>(y, flips, gl);  // (layer 0, table 0) flips come first
+  float v = 0.0f;
+  int c = 0;
+  group_top2_cp<FHT>(y, gl, D, log2D, 1, &v, &c);
+  if (gl == 0 && active) {
+    key[q] = (uint32_t)c;
+    atomicAdd(hist + c, 1u);
+  }
+}
+
+// one block of 1024 threads: counting sort of the keys into `order`; leaves
+// the histogram zeroed for the next batch
+__global__ void __launch_bounds__(1024) k_order_scatter(const uint32_t* __restrict__ key, int nq, int bins,
+                                                        uint32_t* __restrict__ hist, uint32_t* __restrict__ order) {
+  __shared__ uint32_t off[kOrderMaxBins];
+  __shared__ long long tmp[32];
+  const int t = threadIdx.x;
+  const uint32_t h = t < bins ? hist[t] : 0u;
+  long long tot;
+  const long long ex = block_exclusive_scan((long long)h, tmp, &tot);
+  if (t < bins) {
+    off[t] = (uint32_t)ex;
+    hist[t] = 0u;
+  }
+  __syncthreads();
+  for (int q = t; q < nq; q += blockDim.x) order[atomicAdd(&off[key[q]], 1u)] = (uint32_t)q;
+}
+
+static const void* order_key_kernel(int fht) {
+  switch (fht) {
+    case 32: return reinterpret_cast<const void*>(&k_order_key<32>);
+    case 64: return reinterpret_cast<const void*>(&k_order_key<64>);
+    case 128: return reinterpret_cast<const void*>(&k_order_key<128>);
+    case 256: return reinterpret_cast<const void*>(&k_order_key<256>);
+    case 512: return reinterpret_cast<const void*>(&k_order_key<512>);
+    default: return nullptr;
+  }
+}
+
 // ---------------------------------------------------------------- host side
 int ensure_lowp_rows(const Params& P, DeviceIndex& di, int mode, cudaStream_t s, Error& err) {
   if (mode == kRowsF32 || di.lp_mode == mode) return kOk;
@@ -108,6 +170,9 @@ void BatchWorkspace::release() {
   cudaFree(gheap_v);
   cudaFree(gheap_i);
   cudaFree(counters);
+  cudaFree(okey);
+  cudaFree(ohist);
+  cudaFree(order);
   *this = BatchWorkspace();
 }
 
@@ -189,6 +254,36 @@ int batch_query(const Params& P, DeviceIndex& di, BatchWorkspace& bw, const Batc
     bw.mmax = std::max(mmax, 1);
   }
   grid = std::min(grid, bw.grid);
+  // query order (worth it once the batch is a few waves of blocks)
+  int log2D = 0;
+  while ((1 << log2D) < D) ++log2D;
+  const void* okern = order_key_kernel(F);
+  const bool reorder = rq.reorder && okern && rq.nq >= 2 * grid && 2 * D <= kOrderMaxBins;
+  if (reorder && bw.order_cap < rq.nq) {
+    cudaFree(bw.okey);
+    cudaFree(bw.ohist);
+    cudaFree(bw.order);
+    bw.okey = bw.ohist = bw.order = nullptr;
+    bw.order_cap = 0;
+    if ((e = cudaMalloc(&bw.okey, sizeof(uint32_t) * (size_t)rq.nq)) != cudaSuccess) return fail(e, "alloc");
+    if ((e = cudaMalloc(&bw.order, sizeof(uint32_t) * (size_t)rq.nq)) != cudaSuccess) return fail(e, "alloc");
+    if ((e = cudaMalloc(&bw.ohist, sizeof(uint32_t) * kOrderMaxBins)) != cudaSuccess) return fail(e, "alloc");
+    if ((e = cudaMemsetAsync(bw.ohist, 0, sizeof(uint32_t) * kOrderMaxBins, s)) != cudaSuccess)
+      return fail(e, "memset");
+    bw.order_cap = rq.nq;
+  }
+  if (reorder) {
+    const int per_block = 256 / (F / 32);
+    const float* q_ptr = rq.Q;
+    int nq_arg = rq.nq, d_arg = d, D_arg = D, l2_arg = log2D, bins = 2 * D;
+    const uint32_t* fl = di.flips;
+    void* kargs[] = {&q_ptr, &nq_arg, &d_arg, &fl, &D_arg, &l2_arg, &bw.okey, &bw.ohist};
+    if ((e = cudaLaunchKernel(okern, dim3((rq.nq + per_block - 1) / per_block), dim3(256), kargs, 0, s)) !=
+        cudaSuccess)
+      return fail(e, "order key launch");
+    k_order_scatter<<<1, 1024, 0, s>>>(bw.okey, rq.nq, bins, bw.ohist, bw.order);
+    if ((e = cudaGetLastError()) != cudaSuccess) return fail(e, "order scatter launch");
+  }
   BatchArgs a;
   a.Xc = di.Xc;
   a.ld = di.ld;
@@ -213,8 +308,6 @@ int batch_query(const Params& P, DeviceIndex& di, BatchWorkspace& bw, const Batc
   a.d = d;
   a.L = L;
   a.D = D;
-  int log2D = 0;
-  while ((1 << log2D) < D) ++log2D;
   a.log2D = log2D;
   a.NB = 4u * (uint32_t)D * (uint32_t)D;
   a.Q = rq.Q;
@@ -240,12 +333,13 @@ int batch_query(const Params& P, DeviceIndex& di, BatchWorkspace& bw, const Batc
   a.mmax = bw.mmax;
   a.work = bw.counters;
   a.status = bw.counters + 1;
+  a.order = reorder ? bw.order : nullptr;
   void* args[] = {&a};
 
   const bool can_graph = rq.use_graph;
   BatchKey key{rq.Q, rq.nq, rq.q_k, rq.q_qprobes, rq.k_uniform, rq.qprobes_uniform, rq.k_max, rq.qprobes_max,
                rq.shortlist_mult, rq.out,
-               rq.out_stride, rq.out_v, rq.mode, grid, kern, bw.bitset, s};
+               rq.out_stride, rq.out_v, rq.mode, grid, kern, bw.bitset, a.order, s};
   // same launch shape (kernel, grid, stream, scratch): the captured graph is
   // replayed, with the kernel node's arguments updated when they changed
   const bool same_shape = bw.graph_exec && bw.key.kern == key.kern && bw.key.grid == key.grid &&
@@ -300,7 +394,7 @@ int batch_query(const Params& P, DeviceIndex& di, BatchWorkspace& bw, const Batc
         return fail(e, "launch");
     }
   }
-  res.launches = 1;
+  res.launches = reorder ? 3 : 1;
   res.grid = grid;
   if (rq.check_status) {
     unsigned st[2] = {0, 0};

@@ -22,6 +22,7 @@ struct BatchRequest {
   bool use_graph = false;
   bool check_status = true;        // synchronise and report overflow
   int blocks_per_sm = 0;           // 0 = as many as fit
+  bool reorder = true;             // process the queries grouped by a locality key
 };
 
 struct BatchResult {
@@ -44,12 +45,13 @@ struct BatchKey {
   int mode, grid;
   const void* kern;
   uint32_t* bitset;
+  const uint32_t* order;
   cudaStream_t stream;
   bool operator==(const BatchKey& o) const {
     return Q == o.Q && nq == o.nq && q_k == o.q_k && q_qprobes == o.q_qprobes && k_uniform == o.k_uniform &&
            qprobes_uniform == o.qprobes_uniform && k_max == o.k_max && qprobes_max == o.qprobes_max && shortlist_mult == o.shortlist_mult && out == o.out &&
            out_stride == o.out_stride && out_v == o.out_v && mode == o.mode && grid == o.grid && kern == o.kern &&
-           bitset == o.bitset && stream == o.stream;
+           bitset == o.bitset && order == o.order && stream == o.stream;
   }
 };
 
@@ -67,6 +69,11 @@ struct BatchWorkspace {
   int fht = 0;
   int grid = 0;
   unsigned* counters = nullptr;
+  // query order: key per query, histogram of the keys, the permutation
+  uint32_t* okey = nullptr;
+  uint32_t* ohist = nullptr;
+  uint32_t* order = nullptr;
+  long long order_cap = 0;
   cudaGraphExec_t graph_exec = nullptr;
   cudaGraph_t graph = nullptr;
   cudaGraphNode_t graph_knode = nullptr;

@@ -62,6 +62,7 @@ struct BatchArgs {
   int mmax;
   unsigned int* work;
   unsigned int* status;  // bit 0: candidate capacity overflow; bit 1: per-query k/qProbes out of range
+  const uint32_t* order;  // processing order of the queries (nullable: 0, 1, ...)
 };
 
 __device__ __forceinline__ int ceil_sqrt_int(int m) {
@@ -282,7 +283,7 @@ __global__ void __launch_bounds__(kBThreads, MODE == kRowsF32 ? 2 : 3) k_batch_q
     __syncthreads();
     const unsigned qu = s_q;
     if (qu >= (unsigned)a.nq) break;
-    const int q = (int)qu;
+    const int q = a.order ? (int)a.order[qu] : (int)qu;
     const int k = a.q_k ? a.q_k[q] : a.k_uniform;
     const int Qp = a.q_qprobes ? a.q_qprobes[q] : a.qprobes_uniform;
     if (k < 1 || k > a.k_max || Qp < 1 || Qp > a.qprobes_max) {  // block-uniform

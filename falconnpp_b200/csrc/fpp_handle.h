@@ -23,6 +23,7 @@ struct fpp_index {
   int shortlist_mult = 4;   // batched low precision: FP32 re-score of shortlist_mult * k
   bool use_graph = false;   // batched form: capture/replay the launch as a CUDA graph
   int blocks_per_sm = 0;    // batched form: 0 = occupancy limit
+  bool reorder = true;      // batched form: process queries grouped by a locality key
   bool params_set = false;
   bool built = false;
   int device = 0;

@@ -103,7 +103,10 @@ int fpp_get_stats(fpp_index* h, int kind, double* out, int n);
  * "stage_timing" (0/1: CUDA events around each query kernel), "use_graph"
  * (0/1: batched form captured into a CUDA graph and replayed for repeated
  * shapes; the stream must not be the legacy default stream), "blocks_per_sm"
- * (batched form: resident blocks per SM, 0 = occupancy limit). */
+ * (batched form: resident blocks per SM, 0 = occupancy limit),
+ * "reorder_queries" (default 1: the batched form processes a batch grouped by
+ * the first table's first-layer bucket code, so queries in flight together
+ * share buckets and rows in L2; results are unchanged). */
 int fpp_set_option(fpp_index* h, const char* key, long long value);
 
 /* Prints the build report the reference writes to stdout after

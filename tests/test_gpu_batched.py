@@ -107,3 +107,22 @@ def test_low_precision_shortlist(precision):
     for qi in range(0, 500, 50):
         for j in range(20):
             assert val[qi, j] == np.float32(oracle.dot(Q[qi], Xc[ids[qi, j]]))
+
+
+@pytest.mark.parametrize("precision", [0, 1, 2])
+def test_query_order_changes_nothing(precision):
+    # 3000 queries on one block per SM: the batch is a few waves, so the
+    # grouped processing order is used; every query must get the result it
+    # gets in submission order (and, in FP32, the plain path's)
+    X = synth.mixture(20000, 200, seed=0)
+    Q = synth.mixture(3000, 200, seed=1)
+    g = _index(X, 10, 256, 50, 0.01, 3)
+    g.set_qprobes(10)
+    g.set_option("blocks_per_sm", 1)
+    g.set_option("reorder_queries", 0)
+    base = _batched(g, Q, 10, 10, precision=precision)
+    g.set_option("reorder_queries", 1)
+    for graph in (False, True):
+        assert np.array_equal(_batched(g, Q, 10, 10, precision=precision, graph=graph), base), graph
+    if precision == 0:
+        assert np.array_equal(base, g.query(Q, 10))
