@@ -334,12 +334,13 @@ int batch_query(const Params& P, DeviceIndex& di, BatchWorkspace& bw, const Batc
   a.work = bw.counters;
   a.status = bw.counters + 1;
   a.order = reorder ? bw.order : nullptr;
+  a.tflips = (rq.tc_rotation && rq.mode != kRowsF32 && F == 256) ? di.tflips : nullptr;
   void* args[] = {&a};
 
   const bool can_graph = rq.use_graph;
   BatchKey key{rq.Q, rq.nq, rq.q_k, rq.q_qprobes, rq.k_uniform, rq.qprobes_uniform, rq.k_max, rq.qprobes_max,
                rq.shortlist_mult, rq.out,
-               rq.out_stride, rq.out_v, rq.mode, grid, kern, bw.bitset, a.order, s};
+               rq.out_stride, rq.out_v, rq.mode, grid, kern, bw.bitset, a.order, a.tflips, s};
   // same launch shape (kernel, grid, stream, scratch): the captured graph is
   // replayed, with the kernel node's arguments updated when they changed
   const bool same_shape = bw.graph_exec && bw.key.kern == key.kern && bw.key.grid == key.grid &&

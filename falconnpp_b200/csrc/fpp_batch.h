@@ -23,6 +23,7 @@ struct BatchRequest {
   bool check_status = true;        // synchronise and report overflow
   int blocks_per_sm = 0;           // 0 = as many as fit
   bool reorder = true;             // process the queries grouped by a locality key
+  bool tc_rotation = true;         // BF16/FP8, fhtDim 256: rotate on the tensor cores (FP16 operands)
 };
 
 struct BatchResult {
@@ -46,12 +47,13 @@ struct BatchKey {
   const void* kern;
   uint32_t* bitset;
   const uint32_t* order;
+  const uint32_t* tflips;
   cudaStream_t stream;
   bool operator==(const BatchKey& o) const {
     return Q == o.Q && nq == o.nq && q_k == o.q_k && q_qprobes == o.q_qprobes && k_uniform == o.k_uniform &&
            qprobes_uniform == o.qprobes_uniform && k_max == o.k_max && qprobes_max == o.qprobes_max && shortlist_mult == o.shortlist_mult && out == o.out &&
            out_stride == o.out_stride && out_v == o.out_v && mode == o.mode && grid == o.grid && kern == o.kern &&
-           bitset == o.bitset && order == o.order && stream == o.stream;
+           bitset == o.bitset && order == o.order && tflips == o.tflips && stream == o.stream;
   }
 };
 

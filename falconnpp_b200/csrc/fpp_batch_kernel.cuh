@@ -12,6 +12,7 @@
 #include "fpp_batch.h"
 #include "fpp_device.cuh"
 #include "fpp_rows.cuh"
+#include "fpp_tc_rotate.cuh"
 
 namespace fpp {
 
@@ -63,6 +64,7 @@ struct BatchArgs {
   unsigned int* work;
   unsigned int* status;  // bit 0: candidate capacity overflow; bit 1: per-query k/qProbes out of range
   const uint32_t* order;  // processing order of the queries (nullable: 0, 1, ...)
+  const uint32_t* tflips;  // non-null: rotate on the tensor cores when a query keeps one probe per table
 };
 
 __device__ __forceinline__ int ceil_sqrt_int(int m) {
@@ -303,7 +305,7 @@ __global__ void __launch_bounds__(kBThreads, MODE == kRowsF32 ? 2 : 3) k_batch_q
         if (i < G * E) sm.qh[(i >> 5) * kQhStride + (i & 31)] = x;
         amax = fmaxf(amax, fabsf(x));
       }
-      if (MODE == kRowsFP8) {
+      if (MODE != kRowsF32) {
 #pragma unroll
         for (int o = 16; o; o >>= 1) amax = fmaxf(amax, __shfl_xor_sync(kFullMask, amax, o));
         if (lane == 0) atomicMax(&s_qmax, __float_as_uint(amax));  // non-negative: bits order as values
@@ -312,7 +314,38 @@ __global__ void __launch_bounds__(kBThreads, MODE == kRowsF32 ? 2 : 3) k_batch_q
     __syncthreads();
 
     // ---- 1. rotate + hash every table (FalconnPP.cpp:358-531)
-    {
+    if (FHT == 256 && MODE != kRowsF32 && a.tflips && m == 1) {
+      // low-precision modes with one probe per table: each warp rotates one
+      // (table, layer) at a time on the tensor cores and keeps its best
+      // coordinate (ties to the smaller position)
+      float scale = 1.0f;
+      {
+        const float qm = __uint_as_float(s_qmax);
+        int ex = 0;
+        if (qm > 0.0f) {
+          frexpf(qm, &ex);  // qm < 2^ex
+          scale = __int_as_float(min(254, max(1, 123 - ex)) << 23);  // 2^(-ex-4): max |q| * scale < 1/16
+        }
+      }
+      const H16Frags hf(lane);
+      uint32_t qb[2][2];
+      tc_query_frags(sm.q, scale, lane, qb);
+      for (int it = warp; it < 2 * L; it += kBWarps) {
+        const int l = it >> 1, layer = it & 1;
+        float v;
+        int code;
+        tc_rotate_top1(qb, a.tflips + ((size_t)(layer * L + l) * 3) * 8, hf, lane, a.D, a.log2D, &v, &code);
+        if (lane == 0) {
+          sm.gv[it] = v;
+          sm.gc[it] = code;
+        }
+      }
+      __syncthreads();
+      for (int l = tid; l < L; l += kBThreads) {
+        s_lv[l] = __fadd_rn(sm.gv[2 * l], sm.gv[2 * l + 1]);
+        s_lb[l] = (uint32_t)l * a.NB + (uint32_t)(sm.gc[2 * l] * 2 * a.D + sm.gc[2 * l + 1]);
+      }
+    } else {
       const float* xs = sm.qh + gl * kQhStride;  // the query segment of this lane, zero padded past d
       const int cnt = min(m1 + 1, a.D);
       const int rounds = (L + GROUPS - 1) / GROUPS;

@@ -545,6 +545,7 @@ void free_index(DeviceIndex& di) {
   cudaFree(di.Xc);
   cudaFree(di.center);
   cudaFree(di.flips);
+  cudaFree(di.tflips);
   cudaFree(di.bucket_off);
   cudaFree(di.ids);
   cudaFree(di.Xlp);
@@ -589,7 +590,7 @@ int build_index(const Params& P, const float* X, bool x_on_device, const HostBit
   uint64_t ids_capacity = 0;
   int h_bad = 0;
   unsigned long long h_base = 0;
-  std::vector<uint32_t> hflips;
+  std::vector<uint32_t> hflips, htflips;
   long long tables_per_chunk = 0;
   const long long entry_cap = 1LL << 27;
   long long max_entries = 0;
@@ -645,6 +646,24 @@ int build_index(const Params& P, const float* X, bool x_on_device, const HostBit
   }
   FPP_CUDA(cudaMalloc(&di.flips, sizeof(uint32_t) * hflips.size()));
   FPP_CUDA(cudaMemcpyAsync(di.flips, hflips.data(), sizeof(uint32_t) * hflips.size(), cudaMemcpyHostToDevice, s));
+  if (F == 256) {
+    // the tensor-core rotation (batched low-precision form) reads round 2's
+    // signs in the transposed view: bit 16k + n of its words is the sign of
+    // position 16n + k
+    htflips = hflips;
+    for (size_t v = 0; v < (size_t)2 * L; ++v) {
+      const uint32_t* src = hflips.data() + (v * 3 + 1) * WORDS;
+      uint32_t* dst = htflips.data() + (v * 3 + 1) * WORDS;
+      for (int w = 0; w < WORDS; ++w) dst[w] = 0u;
+      for (int pp = 0; pp < 256; ++pp) {
+        const int p0 = 16 * (pp & 15) + (pp >> 4);
+        if ((src[p0 >> 5] >> (p0 & 31)) & 1u) dst[pp >> 5] |= 1u << (pp & 31);
+      }
+    }
+    FPP_CUDA(cudaMalloc(&di.tflips, sizeof(uint32_t) * htflips.size()));
+    FPP_CUDA(cudaMemcpyAsync(di.tflips, htflips.data(), sizeof(uint32_t) * htflips.size(), cudaMemcpyHostToDevice,
+                             s));
+  }
 
   // 3. hash + sort + compact, a chunk of tables at a time
   tables_per_chunk = opt.tables_per_chunk > 0 ? opt.tables_per_chunk

@@ -157,6 +157,7 @@ int run_batched(fpp_index* h, const float* dQ, int nq, int k, int32_t* dout, cud
   rq.use_graph = h->use_graph;
   rq.blocks_per_sm = h->blocks_per_sm;
   rq.reorder = h->reorder;
+  rq.tc_rotation = h->tc_rotation;
   rq.check_status = true;
   fpp::BatchResult res;
   fpp::Error err{0, ""};
@@ -281,6 +282,8 @@ int fpp_set_option(fpp_index* h, const char* key, long long value) {
     h->use_graph = value != 0;
   } else if (!strcmp(key, "reorder_queries")) {
     h->reorder = value != 0;
+  } else if (!strcmp(key, "tc_rotation")) {
+    h->tc_rotation = value != 0;
   } else if (!strcmp(key, "blocks_per_sm")) {
     if (value < 0) return fail(FPP_ERR_INVALID_ARGUMENT, "set_option: blocks_per_sm must be >= 0");
     h->blocks_per_sm = (int)value;
@@ -452,6 +455,7 @@ int fpp_autotune(fpp_index* h, const float* d_queries, int n_queries, int k, dou
     rq.out_stride = k;
     rq.blocks_per_sm = bps;
     rq.reorder = h->reorder;
+    rq.tc_rotation = h->tc_rotation;
     rq.check_status = true;
     fpp::BatchResult res;
     fpp::Error err{0, ""};
@@ -562,6 +566,7 @@ int fpp_query_batched(fpp_index* h, const float* d_queries, int n_queries, const
   rq.use_graph = h->use_graph;
   rq.blocks_per_sm = h->blocks_per_sm;
   rq.reorder = h->reorder;
+  rq.tc_rotation = h->tc_rotation;
   rq.check_status = true;
   fpp::BatchResult res;
   fpp::Error err{0, ""};

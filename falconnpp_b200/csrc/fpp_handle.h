@@ -24,6 +24,7 @@ struct fpp_index {
   bool use_graph = false;   // batched form: capture/replay the launch as a CUDA graph
   int blocks_per_sm = 0;    // batched form: 0 = occupancy limit
   bool reorder = true;      // batched form: process queries grouped by a locality key
+  bool tc_rotation = true;  // batched BF16/FP8 form: tensor-core rotation (fhtDim 256, one probe per table)
   bool params_set = false;
   bool built = false;
   int device = 0;

@@ -51,6 +51,8 @@ struct DeviceIndex {
   int ld = 0;
   float* center = nullptr;           // d floats
   uint32_t* flips = nullptr;         // [2][L][3][words]: 1 = negate (bitHD == 0)
+  uint32_t* tflips = nullptr;        // fhtDim 256 only: the same words per rotation view
+                                     // (round 2 holds the transposed 16 x 16 bit matrix)
   uint32_t* bucket_off = nullptr;    // L*4D^2 + 1 CSR offsets into ids
   int32_t* ids = nullptr;            // stored ids, bucket after bucket
   uint64_t n_ids = 0;

@@ -180,6 +180,7 @@ void worker_loop(fpp_server* S) {
       rq.check_status = false;
       rq.blocks_per_sm = std::max(1, 3 / (int)S->slots.size());
       rq.reorder = h->reorder;
+      rq.tc_rotation = h->tc_rotation;
       fpp::BatchResult res;
       fpp::Error err{0, ""};
       const int rc = fpp::batch_query(h->P, const_cast<fpp::DeviceIndex&>(h->di), s.bw, rq, s.stream, res, err);

@@ -1,0 +1,156 @@
+// fpp_tc_rotate.cuh — HD3 rotation of a 256-point vector on the tensor cores,
+// for the batched form's low-precision modes (the FP32 modes keep the
+// bit-exact FWHT of fpp_device.cuh).
+//
+// The unnormalised FWHT of size 256 in the reference's (Sylvester) order is
+// H256 = H16 (x) H16: with the vector as a 16 x 16 matrix X (x[16a + b] =
+// X[a][b]), FWHT(x) = H16 X H16.  One warp computes one rotation round as two
+// mma.sync m16n8k16 products with FP16 operands and FP32 accumulation:
+//   W = H16 * B   (B = the round's input in B-fragment layout, two n-tiles)
+//   Y = W * H16   (W's accumulator fragment is directly the A fragment)
+// and Y's accumulator fragment, read as a B fragment, is the next round's
+// input transposed (B[k][n] = Y[n][k]); so round 2 works on the transposed
+// view and round 3 on the normal view again.  The sign flips of a round are
+// XOR masks on the packed halves, taken from flip words arranged per view
+// (round 2's words hold the transposed 16 x 16 bit matrix; built with the
+// index).
+//
+// Lane (g, c) = (lane / 4, lane % 4) holds B elements (k, n) = (2c, 2c + 1,
+// 2c + 8, 2c + 9) x (n = 8t + g) for n-tiles t = 0, 1; in the normal view
+// their vector positions are 32c + 8t + g (+16, +128, +144).  The query is
+// scaled by a power of two so that every intermediate stays below 4096 in
+// magnitude (FP16 range); the scale is common to all tables of a query, so
+// comparisons between them are unaffected.
+#pragma once
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace fpp {
+
+__device__ __forceinline__ void mma_f16_m16n8k16(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+  asm("mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+__device__ __forceinline__ uint32_t pack_f16x2(float lo, float hi) {
+  const __half2 h = __floats2half2_rn(lo, hi);
+  return *reinterpret_cast<const uint32_t*>(&h);
+}
+
+// +-1 of H16[i][j] = (-1)^popc(i & j) as two packed halves
+__device__ __forceinline__ uint32_t h16_pair(int i0, int j0, int i1, int j1) {
+  const uint32_t lo = (__popc(i0 & j0) & 1) ? 0xBC00u : 0x3C00u;
+  const uint32_t hi = (__popc(i1 & j1) & 1) ? 0xBC00u : 0x3C00u;
+  return lo | (hi << 16);
+}
+
+// the lane's constant fragments of H16: as the A operand, and as the B
+// operand of n-tiles 0 and 1
+struct H16Frags {
+  uint32_t a[4];
+  uint32_t b[2][2];
+  __device__ explicit H16Frags(int lane) {
+    const int g = lane >> 2, c = lane & 3;
+    a[0] = h16_pair(g, 2 * c, g, 2 * c + 1);
+    a[1] = h16_pair(g + 8, 2 * c, g + 8, 2 * c + 1);
+    a[2] = h16_pair(g, 2 * c + 8, g, 2 * c + 9);
+    a[3] = h16_pair(g + 8, 2 * c + 8, g + 8, 2 * c + 9);
+#pragma unroll
+    for (int t = 0; t < 2; ++t) {
+      b[t][0] = h16_pair(2 * c, 8 * t + g, 2 * c + 1, 8 * t + g);
+      b[t][1] = h16_pair(2 * c + 8, 8 * t + g, 2 * c + 9, 8 * t + g);
+    }
+  }
+};
+
+// the scaled query as the lane's round-1 B registers (normal view)
+__device__ __forceinline__ void tc_query_frags(const float* q, float scale, int lane, uint32_t (&qb)[2][2]) {
+  const int g = lane >> 2, c = lane & 3;
+#pragma unroll
+  for (int t = 0; t < 2; ++t) {
+    const int p = 32 * c + 8 * t + g;
+    qb[t][0] = pack_f16x2(q[p] * scale, q[p + 16] * scale);
+    qb[t][1] = pack_f16x2(q[p + 128] * scale, q[p + 144] * scale);
+  }
+}
+
+// Three rounds (sign flip, FWHT-256) of the lane's fragments starting from
+// qb; tw = the 3 x 8 flip words of this (layer, table) in per-view order.
+// Returns the best cross-polytope coordinate among positions < D: its value
+// sgn(y)*y, and its bucket code (position | (y < 0) << log2D), ties to the
+// smaller position; the same on every lane.
+__device__ __forceinline__ void tc_rotate_top1(const uint32_t (&qb)[2][2], const uint32_t* __restrict__ tw,
+                                               const H16Frags& h, int lane, int D, int log2D, float* best_v,
+                                               int* best_code) {
+  const int g = lane >> 2, c = lane & 3;
+  uint32_t b[2][2] = {{qb[0][0], qb[0][1]}, {qb[1][0], qb[1][1]}};
+  uint32_t wl[3], wh[3];
+#pragma unroll
+  for (int r = 0; r < 3; ++r) {
+    wl[r] = __ldg(tw + r * 8 + c);
+    wh[r] = __ldg(tw + r * 8 + c + 4);
+  }
+  float y[2][4];
+#pragma unroll
+  for (int r = 0; r < 3; ++r) {
+    // sign flips: bits s and s + 16 of words c and c + 4 (s = 8t + g) go to
+    // the sign bits 15 and 31 of the packed pair
+#pragma unroll
+    for (int t = 0; t < 2; ++t) {
+      const int sh = 15 - (8 * t + g);
+      b[t][0] ^= (wl[r] << sh) & 0x80008000u;
+      b[t][1] ^= (wh[r] << sh) & 0x80008000u;
+    }
+    float w[2][4];
+#pragma unroll
+    for (int t = 0; t < 2; ++t) {
+      w[t][0] = w[t][1] = w[t][2] = w[t][3] = 0.0f;
+      mma_f16_m16n8k16(w[t], h.a, b[t][0], b[t][1]);
+    }
+    const uint32_t a[4] = {pack_f16x2(w[0][0], w[0][1]), pack_f16x2(w[0][2], w[0][3]),
+                           pack_f16x2(w[1][0], w[1][1]), pack_f16x2(w[1][2], w[1][3])};
+#pragma unroll
+    for (int t = 0; t < 2; ++t) {
+      y[t][0] = y[t][1] = y[t][2] = y[t][3] = 0.0f;
+      mma_f16_m16n8k16(y[t], a, h.b[t][0], h.b[t][1]);
+    }
+    if (r < 2) {
+      b[0][0] = pack_f16x2(y[0][0], y[0][1]);
+      b[0][1] = pack_f16x2(y[1][0], y[1][1]);
+      b[1][0] = pack_f16x2(y[0][2], y[0][3]);
+      b[1][1] = pack_f16x2(y[1][2], y[1][3]);
+    }
+  }
+  // y[t][e] is Y[g + 8 (e >> 1)][8t + 2c + (e & 1)], position 16 * row + col
+  float bv = -1.0f, by = 0.0f;
+  int bp = 0x7fffffff;
+#pragma unroll
+  for (int t = 0; t < 2; ++t)
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const int pos = 16 * (g + 8 * (e >> 1)) + 8 * t + 2 * c + (e & 1);
+      const float v = y[t][e] >= 0.0f ? y[t][e] : -y[t][e];
+      if (pos < D && (v > bv || (v == bv && pos < bp))) {
+        bv = v;
+        bp = pos;
+        by = y[t][e];
+      }
+    }
+#pragma unroll
+  for (int o = 16; o; o >>= 1) {
+    const float ov = __shfl_xor_sync(0xffffffffu, bv, o);
+    const int op = __shfl_xor_sync(0xffffffffu, bp, o);
+    const float oy = __shfl_xor_sync(0xffffffffu, by, o);
+    if (ov > bv || (ov == bv && op < bp)) {
+      bv = ov;
+      bp = op;
+      by = oy;
+    }
+  }
+  *best_v = bv;
+  *best_code = by >= 0.0f ? bp : (bp | (1 << log2D));
+}
+
+}  // namespace fpp

@@ -106,7 +106,11 @@ int fpp_get_stats(fpp_index* h, int kind, double* out, int n);
  * (batched form: resident blocks per SM, 0 = occupancy limit),
  * "reorder_queries" (default 1: the batched form processes a batch grouped by
  * the first table's first-layer bucket code, so queries in flight together
- * share buckets and rows in L2; results are unchanged). */
+ * share buckets and rows in L2; results are unchanged), "tc_rotation"
+ * (default 1: the batched BF16/FP8 form with fhtDim 256 and one probe per
+ * table rotates on the tensor cores with FP16 operands and FP32 accumulation;
+ * its probes can differ from the exact FP32 rotation's where two rotated
+ * coordinates or two bucket scores are within about 1e-3 of each other). */
 int fpp_set_option(fpp_index* h, const char* key, long long value);
 
 /* Prints the build report the reference writes to stdout after

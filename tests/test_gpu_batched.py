@@ -126,3 +126,32 @@ def test_query_order_changes_nothing(precision):
         assert np.array_equal(_batched(g, Q, 10, 10, precision=precision, graph=graph), base), graph
     if precision == 0:
         assert np.array_equal(base, g.query(Q, 10))
+
+
+@pytest.mark.parametrize("precision", [1, 2])
+def test_tensor_core_rotation(precision):
+    # fhtDim 256 and one probe per table (qProbes <= L / 2): the low-precision
+    # modes rotate on the tensor cores with FP16 operands.  Probes may differ
+    # from the exact rotation's only on near-ties, so the ids agree with the
+    # exact-rotation result almost everywhere, recall against the plain path
+    # stays high, and the returned scores are still exact FP32 dots.
+    X = synth.mixture(50000, 200, seed=0)
+    Q = synth.mixture(1000, 200, seed=1)
+    g = _index(X, 40, 256, 100, 0.01, 3)
+    g.set_qprobes(10)
+    exact = g.query(Q, 20)
+    g.set_option("tc_rotation", 0)
+    ref_ids = _batched(g, Q, 20, 10, precision=precision, mult=4)
+    g.set_option("tc_rotation", 1)
+    ids, val = _batched(g, Q, 20, 10, precision=precision, mult=4, with_val=True)
+    agree = np.mean([len(set(a) & set(b)) / 20 for a, b in zip(ref_ids.tolist(), ids.tolist())])
+    assert agree >= 0.95, agree
+    rec = synth.recall_at_k(exact, ids, 20)
+    assert rec >= 0.95, rec
+    from oracle import oracle
+    mean, Xc = oracle.center(X)
+    for qi in range(0, 1000, 100):
+        for j in range(20):
+            assert val[qi, j] == np.float32(oracle.dot(Q[qi], Xc[ids[qi, j]]))
+    # the same batch again gives the same ids (the rotation is deterministic)
+    assert np.array_equal(_batched(g, Q, 20, 10, precision=precision, mult=4), ids)
