@@ -680,14 +680,35 @@ __global__ void __launch_bounds__(kBThreads, MODE == kRowsF32 ? 2 : 3) k_batch_q
                                     (size_t)a.ld * 4, a.ld / 4, nullptr, warp, kBWarps, lane, nullptr);
         __syncthreads();
       }
-      for (unsigned i = tid; i < nsel; i += kBThreads)
-        s_top[i] = ((unsigned long long)(~ord_key_bits(ssc[i])) << 32) | sid[i];
-      __syncthreads();
-      block_sort_u64(s_top, (int)nsel);
       const unsigned kept = min(nsel, kk);
       unsigned dup = 0;
-      // equal FP32 scores in the kept list, or at the k-th place: heap order decides
-      for (unsigned i = tid; i + 1 < nsel && i < kk; i += kBThreads) dup |= (s_top[i] >> 32) == (s_top[i + 1] >> 32);
+      // s_top[0..kept): the best candidates by (score desc, id asc).  Equal
+      // FP32 scores in the kept list, or at the k-th place, leave the order to
+      // the reference's heap (dup).
+      if (nsel <= 2u * kBThreads) {
+        // rank by counting: no sort, two barriers
+        for (unsigned i = tid; i < nsel; i += kBThreads) {
+          const uint32_t ki = ord_key_bits(ssc[i]);
+          const uint32_t ii = sid[i];
+          unsigned gt = 0, eq = 0, before = 0;
+          for (unsigned j = 0; j < nsel; ++j) {
+            const uint32_t kj = ord_key_bits(ssc[j]);
+            gt += kj > ki;
+            eq += kj == ki;
+            before += (kj == ki) & (sid[j] < ii);
+          }
+          const unsigned r = gt + before;
+          if (r < kept) s_top[r] = ((unsigned long long)(~ki) << 32) | ii;
+          dup |= (eq > 1u) & (gt < kk);
+        }
+      } else {
+        for (unsigned i = tid; i < nsel; i += kBThreads)
+          s_top[i] = ((unsigned long long)(~ord_key_bits(ssc[i])) << 32) | sid[i];
+        __syncthreads();
+        block_sort_u64(s_top, (int)nsel);
+        for (unsigned i = tid; i + 1 < nsel && i < kk; i += kBThreads)
+          dup |= (s_top[i] >> 32) == (s_top[i + 1] >> 32);
+      }
       exact = !__syncthreads_or(dup);
       if (exact) {
         for (int j = tid; j < k; j += kBThreads) {
@@ -710,9 +731,9 @@ __global__ void __launch_bounds__(kBThreads, MODE == kRowsF32 ? 2 : 3) k_batch_q
       uint32_t* cid = uq;
       uint32_t* csc = sc;
       if (!whole) {
-        for (unsigned i = tid; i < nc; i += kBThreads) {
-          cid[i] = (uint32_t)s_top[i];
-          csc[i] = ord_key_inv_dev(~(uint32_t)(s_top[i] >> 32));
+        for (unsigned i = tid; i < nc; i += kBThreads) {  // the shortlist with its exact FP32 scores
+          cid[i] = sid[i];
+          csc[i] = ssc[i];
         }
         __syncthreads();
         if (use_bitset) {  // the unique list was overwritten: clear every word

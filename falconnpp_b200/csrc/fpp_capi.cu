@@ -141,8 +141,12 @@ void print_build(const fpp_index* h) {
             << " seconds" << std::endl;
 }
 
-// Runs the batched form for device queries/outputs (uniform k, the handle's qProbes).
-int run_batched(fpp_index* h, const float* dQ, int nq, int k, int32_t* dout, cudaStream_t s) {
+// Runs the batched form for device queries/outputs (uniform k, the handle's
+// qProbes).  With check_status false the call does not wait for the kernel;
+// the caller reads the status words (h->bw.counters + 1) after its own copies
+// and reports an overflow with batched_overflow_error().
+int run_batched(fpp_index* h, const float* dQ, int nq, int k, int32_t* dout, cudaStream_t s,
+                bool check_status = true) {
   fpp::BatchRequest rq;
   rq.Q = dQ;
   rq.nq = nq;
@@ -158,7 +162,7 @@ int run_batched(fpp_index* h, const float* dQ, int nq, int k, int32_t* dout, cud
   rq.blocks_per_sm = h->blocks_per_sm;
   rq.reorder = h->reorder;
   rq.tc_rotation = h->tc_rotation;
-  rq.check_status = true;
+  rq.check_status = check_status;
   fpp::BatchResult res;
   fpp::Error err{0, ""};
   const int rc = fpp::batch_query(h->P, h->di, h->bw, rq, s, res, err);
@@ -353,11 +357,16 @@ int fpp_query(fpp_index* h, const float* queries, int n_queries, int n_neighbors
     }
     if (e != cudaSuccess) return fail(FPP_ERR_OUT_OF_MEMORY, std::string("query: ") + cudaGetErrorString(e));
     cudaMemcpyAsync(h->ws.Qd, queries, sizeof(float) * n_queries * P.n_features, cudaMemcpyHostToDevice, h->stream);
-    rc = run_batched(h, h->ws.Qd, n_queries, n_neighbors, h->ws.out, h->stream);
+    // one synchronisation: results and the kernel's status words come back together
+    rc = run_batched(h, h->ws.Qd, n_queries, n_neighbors, h->ws.out, h->stream, false);
     if (rc) return rc;
+    unsigned status = 0;
     e = cudaMemcpyAsync(out, h->ws.out, sizeof(int32_t) * n_queries * n_neighbors, cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(&status, h->bw.counters + 1, sizeof(unsigned), cudaMemcpyDeviceToHost, h->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
     if (e != cudaSuccess) return fail(FPP_ERR_CUDA, std::string("query: ") + cudaGetErrorString(e));
+    if (status & 1u) return fail(FPP_ERR_UNSUPPORTED, "batched query: candidate capacity exceeded");
   } else {
     rc = fpp::query_index(P, h->di, queries, false, n_queries, n_neighbors, out, false, h->ws, h->qst, h->stream,
                           err, nullptr);
