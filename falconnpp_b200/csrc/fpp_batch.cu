@@ -176,11 +176,11 @@ void BatchWorkspace::release() {
   *this = BatchWorkspace();
 }
 
-static KernelSel pick_kernel(int fht, int mode, int d) {
+static KernelSel pick_kernel(int fht, int mode, int d, bool tc_only) {
   if (d > 512) return KernelSel{nullptr, 0};
   if (mode == kRowsF32) return pick_kernel_f32(fht, d);
-  if (mode == kRowsBF16) return pick_kernel_bf16(fht, d);
-  return pick_kernel_fp8(fht, d);
+  if (mode == kRowsBF16) return pick_kernel_bf16(fht, d, tc_only);
+  return pick_kernel_fp8(fht, d, tc_only);
 }
 
 int batch_query(const Params& P, DeviceIndex& di, BatchWorkspace& bw, const BatchRequest& rq, cudaStream_t s,
@@ -211,7 +211,10 @@ int batch_query(const Params& P, DeviceIndex& di, BatchWorkspace& bw, const Batc
     const int rc = ensure_lowp_rows(P, di, rq.mode, s, err);
     if (rc) return rc;
   }
-  const KernelSel ks = pick_kernel(F, rq.mode, d);
+  // every query keeps one probe per table (2 qProbes <= L): the kernel
+  // without the exact rotation
+  const bool tc_only = rq.tc_rotation && rq.mode != kRowsF32 && F == 256 && di.tflips && 2 * rq.qprobes_max <= L;
+  const KernelSel ks = pick_kernel(F, rq.mode, d, tc_only);
   const void* kern = ks.fn;
   if (!kern) {
     err.code = kErrUnsupported;

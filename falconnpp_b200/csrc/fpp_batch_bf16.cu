@@ -3,9 +3,14 @@
 
 namespace fpp {
 
-KernelSel pick_kernel_bf16(int fht, int d) {
+KernelSel pick_kernel_bf16(int fht, int d, bool tc_only) {
   // the first rerank runs on the tensor cores (VI unused); VI32 sizes the FP32 re-score
   const int v32 = vi_of(d, 4);
+  if (tc_only && fht == 256) {
+    if (v32 == 1) return kernel_ptr<256, kRowsBF16, 1, 1, kHashTC>();
+    if (v32 == 2) return kernel_ptr<256, kRowsBF16, 1, 2, kHashTC>();
+    return kernel_ptr<256, kRowsBF16, 1, 4, kHashTC>();
+  }
   if (v32 == 1) return pick_fht<kRowsBF16, 1, 1>(fht);
   if (v32 == 2) return pick_fht<kRowsBF16, 1, 2>(fht);
   if (v32 == 4) return pick_fht<kRowsBF16, 1, 4>(fht);

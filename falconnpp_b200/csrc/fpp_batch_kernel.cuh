@@ -243,8 +243,15 @@ constexpr size_t batch_smem_bytes() {
 
 __device__ __forceinline__ uint32_t ht_slot(uint32_t id) { return (id * 2654435761u) >> (32 - 13); }
 
-template <int FHT, int MODE, int VI, int VI32>
+// HASH: kHashAuto rotates on the tensor cores where a query keeps one probe
+// per table (and a.tflips is set), exactly otherwise; kHashTC only on the
+// tensor cores (the host uses it when every query of the batch keeps one
+// probe per table), which leaves the exact rotation's registers out.
+enum HashKind : int { kHashAuto = 0, kHashTC = 1 };
+
+template <int FHT, int MODE, int VI, int VI32, int HASH = kHashAuto>
 __global__ void __launch_bounds__(kBThreads, MODE == kRowsF32 ? 2 : 3) k_batch_query(BatchArgs a) {
+  static_assert(HASH == kHashAuto || (FHT == 256 && MODE != kRowsF32), "tensor-core rotation: fhtDim 256, BF16/FP8");
   constexpr int E = Geo<FHT>::E;
   constexpr int G = Geo<FHT>::G;
   constexpr int WORDS = Geo<FHT>::WORDS;
@@ -314,7 +321,7 @@ __global__ void __launch_bounds__(kBThreads, MODE == kRowsF32 ? 2 : 3) k_batch_q
     __syncthreads();
 
     // ---- 1. rotate + hash every table (FalconnPP.cpp:358-531)
-    if (FHT == 256 && MODE != kRowsF32 && a.tflips && m == 1) {
+    if (FHT == 256 && MODE != kRowsF32 && (HASH == kHashTC || (a.tflips && m == 1))) {
       // low-precision modes with one probe per table: each warp rotates one
       // (table, layer) at a time on the tensor cores and keeps its best
       // coordinate (ties to the smaller position)
@@ -345,7 +352,7 @@ __global__ void __launch_bounds__(kBThreads, MODE == kRowsF32 ? 2 : 3) k_batch_q
         s_lv[l] = __fadd_rn(sm.gv[2 * l], sm.gv[2 * l + 1]);
         s_lb[l] = (uint32_t)l * a.NB + (uint32_t)(sm.gc[2 * l] * 2 * a.D + sm.gc[2 * l + 1]);
       }
-    } else {
+    } else if constexpr (HASH == kHashAuto) {
       const float* xs = sm.qh + gl * kQhStride;  // the query segment of this lane, zero padded past d
       const int cnt = min(m1 + 1, a.D);
       const int rounds = (L + GROUPS - 1) / GROUPS;
@@ -772,9 +779,9 @@ struct KernelSel {
   size_t smem;
 };
 
-template <int FHT, int MODE, int VI, int VI32>
+template <int FHT, int MODE, int VI, int VI32, int HASH = kHashAuto>
 static KernelSel kernel_ptr() {
-  const void* fn = reinterpret_cast<const void*>(&k_batch_query<FHT, MODE, VI, VI32>);
+  const void* fn = reinterpret_cast<const void*>(&k_batch_query<FHT, MODE, VI, VI32, HASH>);
   const size_t smem = batch_smem_bytes<FHT>();
   cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   return KernelSel{fn, smem};
@@ -795,8 +802,8 @@ static KernelSel pick_fht(int fht) {
 // per-precision selection (VI: 16-byte chunks per virtual lane of the FP32
 // first rerank; VI32: of the FP32 re-score), defined in fpp_batch_{f32,bf16,fp8}.cu
 KernelSel pick_kernel_f32(int fht, int d);
-KernelSel pick_kernel_bf16(int fht, int d);
-KernelSel pick_kernel_fp8(int fht, int d);
+KernelSel pick_kernel_bf16(int fht, int d, bool tc_only);
+KernelSel pick_kernel_fp8(int fht, int d, bool tc_only);
 
 inline int vi_of(int d, int epc) {
   const int v = ((d + epc - 1) / epc + 31) / 32;
