@@ -337,14 +337,20 @@ __global__ void __launch_bounds__(kBThreads, MODE == kRowsF32 ? 2 : 3) k_batch_q
       const H16Frags hf(lane);
       uint32_t qb[2][2];
       tc_query_frags(sm.q, scale, lane, qb);
-      for (int it = warp; it < 2 * L; it += kBWarps) {
-        const int l = it >> 1, layer = it & 1;
-        float v;
-        int code;
-        tc_rotate_top1(qb, a.tflips + ((size_t)(layer * L + l) * 3) * 8, hf, lane, a.D, a.log2D, &v, &code);
+      // two (table, layer) items per warp at a time: item it and it + kBWarps
+      // (an item past the end repeats the first, and its result is dropped)
+      for (int it = warp; it < 2 * L; it += 2 * kBWarps) {
+        const int it2 = it + kBWarps < 2 * L ? it + kBWarps : it;
+        const uint32_t* const tw[2] = {a.tflips + ((size_t)((it & 1) * L + (it >> 1)) * 3) * 8,
+                                       a.tflips + ((size_t)((it2 & 1) * L + (it2 >> 1)) * 3) * 8};
+        float v[2];
+        int code[2];
+        tc_rotate_top1<2>(qb, tw, hf, lane, a.D, a.log2D, v, code);
         if (lane == 0) {
-          sm.gv[it] = v;
-          sm.gc[it] = code;
+          sm.gv[it] = v[0];
+          sm.gc[it] = code[0];
+          sm.gv[it2] = v[1];
+          sm.gc[it2] = code[1];
         }
       }
       __syncthreads();

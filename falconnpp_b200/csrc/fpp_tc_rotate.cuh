@@ -77,80 +77,112 @@ __device__ __forceinline__ void tc_query_frags(const float* q, float scale, int 
 }
 
 // Three rounds (sign flip, FWHT-256) of the lane's fragments starting from
-// qb; tw = the 3 x 8 flip words of this (layer, table) in per-view order.
-// Returns the best cross-polytope coordinate among positions < D: its value
+// qb, for NI (table, layer) items at once (independent chains, interleaved);
+// tw[i] = the 3 x 8 flip words of item i in per-view order.  For each item,
+// the best cross-polytope coordinate among positions < D: its value
 // sgn(y)*y, and its bucket code (position | (y < 0) << log2D), ties to the
 // smaller position; the same on every lane.
-__device__ __forceinline__ void tc_rotate_top1(const uint32_t (&qb)[2][2], const uint32_t* __restrict__ tw,
-                                               const H16Frags& h, int lane, int D, int log2D, float* best_v,
-                                               int* best_code) {
+template <int NI>
+__device__ __forceinline__ void tc_rotate_top1(const uint32_t (&qb)[2][2], const uint32_t* const (&tw)[NI],
+                                               const H16Frags& h, int lane, int D, int log2D, float (&best_v)[NI],
+                                               int (&best_code)[NI]) {
   const int g = lane >> 2, c = lane & 3;
-  uint32_t b[2][2] = {{qb[0][0], qb[0][1]}, {qb[1][0], qb[1][1]}};
-  uint32_t wl[3], wh[3];
+  uint32_t b[NI][2][2];
+  uint32_t wl[NI][3], wh[NI][3];
 #pragma unroll
-  for (int r = 0; r < 3; ++r) {
-    wl[r] = __ldg(tw + r * 8 + c);
-    wh[r] = __ldg(tw + r * 8 + c + 4);
+  for (int i = 0; i < NI; ++i) {
+#pragma unroll
+    for (int t = 0; t < 2; ++t) {
+      b[i][t][0] = qb[t][0];
+      b[i][t][1] = qb[t][1];
+    }
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+      wl[i][r] = __ldg(tw[i] + r * 8 + c);
+      wh[i][r] = __ldg(tw[i] + r * 8 + c + 4);
+    }
   }
-  float y[2][4];
+  float y[NI][2][4];
 #pragma unroll
   for (int r = 0; r < 3; ++r) {
     // sign flips: bits s and s + 16 of words c and c + 4 (s = 8t + g) go to
     // the sign bits 15 and 31 of the packed pair
 #pragma unroll
-    for (int t = 0; t < 2; ++t) {
-      const int sh = 15 - (8 * t + g);
-      b[t][0] ^= (wl[r] << sh) & 0x80008000u;
-      b[t][1] ^= (wh[r] << sh) & 0x80008000u;
-    }
-    float w[2][4];
+    for (int i = 0; i < NI; ++i)
 #pragma unroll
-    for (int t = 0; t < 2; ++t) {
-      w[t][0] = w[t][1] = w[t][2] = w[t][3] = 0.0f;
-      mma_f16_m16n8k16(w[t], h.a, b[t][0], b[t][1]);
-    }
-    const uint32_t a[4] = {pack_f16x2(w[0][0], w[0][1]), pack_f16x2(w[0][2], w[0][3]),
-                           pack_f16x2(w[1][0], w[1][1]), pack_f16x2(w[1][2], w[1][3])};
+      for (int t = 0; t < 2; ++t) {
+        const int sh = 15 - (8 * t + g);
+        b[i][t][0] ^= (wl[i][r] << sh) & 0x80008000u;
+        b[i][t][1] ^= (wh[i][r] << sh) & 0x80008000u;
+      }
+    float w[NI][2][4];
 #pragma unroll
-    for (int t = 0; t < 2; ++t) {
-      y[t][0] = y[t][1] = y[t][2] = y[t][3] = 0.0f;
-      mma_f16_m16n8k16(y[t], a, h.b[t][0], h.b[t][1]);
+    for (int i = 0; i < NI; ++i)
+#pragma unroll
+      for (int t = 0; t < 2; ++t) {
+        w[i][t][0] = w[i][t][1] = w[i][t][2] = w[i][t][3] = 0.0f;
+        mma_f16_m16n8k16(w[i][t], h.a, b[i][t][0], b[i][t][1]);
+      }
+#pragma unroll
+    for (int i = 0; i < NI; ++i) {
+      const uint32_t a[4] = {pack_f16x2(w[i][0][0], w[i][0][1]), pack_f16x2(w[i][0][2], w[i][0][3]),
+                             pack_f16x2(w[i][1][0], w[i][1][1]), pack_f16x2(w[i][1][2], w[i][1][3])};
+#pragma unroll
+      for (int t = 0; t < 2; ++t) {
+        y[i][t][0] = y[i][t][1] = y[i][t][2] = y[i][t][3] = 0.0f;
+        mma_f16_m16n8k16(y[i][t], a, h.b[t][0], h.b[t][1]);
+      }
     }
     if (r < 2) {
-      b[0][0] = pack_f16x2(y[0][0], y[0][1]);
-      b[0][1] = pack_f16x2(y[1][0], y[1][1]);
-      b[1][0] = pack_f16x2(y[0][2], y[0][3]);
-      b[1][1] = pack_f16x2(y[1][2], y[1][3]);
+#pragma unroll
+      for (int i = 0; i < NI; ++i) {
+        b[i][0][0] = pack_f16x2(y[i][0][0], y[i][0][1]);
+        b[i][0][1] = pack_f16x2(y[i][1][0], y[i][1][1]);
+        b[i][1][0] = pack_f16x2(y[i][0][2], y[i][0][3]);
+        b[i][1][1] = pack_f16x2(y[i][1][2], y[i][1][3]);
+      }
     }
   }
-  // y[t][e] is Y[g + 8 (e >> 1)][8t + 2c + (e & 1)], position 16 * row + col
-  float bv = -1.0f, by = 0.0f;
-  int bp = 0x7fffffff;
+  // y[i][t][e] is Y[g + 8 (e >> 1)][8t + 2c + (e & 1)], position 16 * row + col
+  float bv[NI], by[NI];
+  int bp[NI];
 #pragma unroll
-  for (int t = 0; t < 2; ++t)
+  for (int i = 0; i < NI; ++i) {
+    bv[i] = -1.0f;
+    by[i] = 0.0f;
+    bp[i] = 0x7fffffff;
 #pragma unroll
-    for (int e = 0; e < 4; ++e) {
-      const int pos = 16 * (g + 8 * (e >> 1)) + 8 * t + 2 * c + (e & 1);
-      const float v = y[t][e] >= 0.0f ? y[t][e] : -y[t][e];
-      if (pos < D && (v > bv || (v == bv && pos < bp))) {
-        bv = v;
-        bp = pos;
-        by = y[t][e];
+    for (int t = 0; t < 2; ++t)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int pos = 16 * (g + 8 * (e >> 1)) + 8 * t + 2 * c + (e & 1);
+        const float yv = y[i][t][e];
+        const float v = yv >= 0.0f ? yv : -yv;
+        if (pos < D && (v > bv[i] || (v == bv[i] && pos < bp[i]))) {
+          bv[i] = v;
+          bp[i] = pos;
+          by[i] = yv;
+        }
+      }
+  }
+#pragma unroll
+  for (int o = 16; o; o >>= 1)
+#pragma unroll
+    for (int i = 0; i < NI; ++i) {
+      const float ov = __shfl_xor_sync(0xffffffffu, bv[i], o);
+      const int op = __shfl_xor_sync(0xffffffffu, bp[i], o);
+      const float oy = __shfl_xor_sync(0xffffffffu, by[i], o);
+      if (ov > bv[i] || (ov == bv[i] && op < bp[i])) {
+        bv[i] = ov;
+        bp[i] = op;
+        by[i] = oy;
       }
     }
 #pragma unroll
-  for (int o = 16; o; o >>= 1) {
-    const float ov = __shfl_xor_sync(0xffffffffu, bv, o);
-    const int op = __shfl_xor_sync(0xffffffffu, bp, o);
-    const float oy = __shfl_xor_sync(0xffffffffu, by, o);
-    if (ov > bv || (ov == bv && op < bp)) {
-      bv = ov;
-      bp = op;
-      by = oy;
-    }
+  for (int i = 0; i < NI; ++i) {
+    best_v[i] = bv[i];
+    best_code[i] = by[i] >= 0.0f ? bp[i] : (bp[i] | (1 << log2D));
   }
-  *best_v = bv;
-  *best_code = by >= 0.0f ? bp : (bp | (1 << log2D));
 }
 
 }  // namespace fpp
