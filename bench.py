@@ -50,7 +50,7 @@ FORM_SPECS = {
     "plain-fp32": (0, 0, 4),
     "batched-fp32": (1, 0, 4),
     "batched-bf16": (1, 1, 2),
-    "batched-fp8": (1, 2, 4),
+    "batched-fp8": (1, 2, 2),
 }
 FORMS = ["plain-fp32", "batched-fp32", "batched-bf16", "batched-fp8"]
 RECALL_SAMPLE = 500
@@ -259,7 +259,7 @@ def run_ours(args, w, rank, world, local_rank):
     # end to end through the C ABI with pinned host buffers (same form)
     Qh = torch.from_numpy(Q).pin_memory()
     outh = torch.empty((nq, k), dtype=torch.int32).pin_memory()
-    for _ in range(max(1, args.warmup // 2)):
+    for _ in range(max(1, args.warmup)):
         capi.lib().fpp_query(idx.h, Qh.data_ptr(), nq, k, 0, outh.data_ptr())
     if dist:
         dist.barrier()
