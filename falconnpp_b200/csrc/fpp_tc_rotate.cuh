@@ -28,10 +28,11 @@
 
 namespace fpp {
 
+// d = A * B with a zero accumulator (no registers to clear beforehand)
 __device__ __forceinline__ void mma_f16_m16n8k16(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
-  asm("mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
-      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+  asm("mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%10,%10,%10,%10};\n"
+      : "=f"(d[0]), "=f"(d[1]), "=f"(d[2]), "=f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1), "f"(0.0f));
 }
 
 __device__ __forceinline__ uint32_t pack_f16x2(float lo, float hi) {
@@ -80,8 +81,9 @@ __device__ __forceinline__ void tc_query_frags(const float* q, float scale, int 
 // qb, for NI (table, layer) items at once (independent chains, interleaved);
 // tw[i] = the 3 x 8 flip words of item i in per-view order.  For each item,
 // the best cross-polytope coordinate among positions < D: its value
-// sgn(y)*y, and its bucket code (position | (y < 0) << log2D), ties to the
-// smaller position; the same on every lane.
+// sgn(y)*y (low 9 mantissa bits cleared), and its bucket code (position |
+// (y < 0) << log2D), equal values to the smaller position; the same on every
+// lane.
 template <int NI>
 __device__ __forceinline__ void tc_rotate_top1(const uint32_t (&qb)[2][2], const uint32_t* const (&tw)[NI],
                                                const H16Frags& h, int lane, int D, int log2D, float (&best_v)[NI],
@@ -120,7 +122,6 @@ __device__ __forceinline__ void tc_rotate_top1(const uint32_t (&qb)[2][2], const
     for (int i = 0; i < NI; ++i)
 #pragma unroll
       for (int t = 0; t < 2; ++t) {
-        w[i][t][0] = w[i][t][1] = w[i][t][2] = w[i][t][3] = 0.0f;
         mma_f16_m16n8k16(w[i][t], h.a, b[i][t][0], b[i][t][1]);
       }
 #pragma unroll
@@ -129,7 +130,6 @@ __device__ __forceinline__ void tc_rotate_top1(const uint32_t (&qb)[2][2], const
                              pack_f16x2(w[i][1][0], w[i][1][1]), pack_f16x2(w[i][1][2], w[i][1][3])};
 #pragma unroll
       for (int t = 0; t < 2; ++t) {
-        y[i][t][0] = y[i][t][1] = y[i][t][2] = y[i][t][3] = 0.0f;
         mma_f16_m16n8k16(y[i][t], a, h.b[t][0], h.b[t][1]);
       }
     }
@@ -143,45 +143,42 @@ __device__ __forceinline__ void tc_rotate_top1(const uint32_t (&qb)[2][2], const
       }
     }
   }
-  // y[i][t][e] is Y[g + 8 (e >> 1)][8t + 2c + (e & 1)], position 16 * row + col
-  float bv[NI], by[NI];
-  int bp[NI];
+  // y[i][t][e] is Y[g + 8 (e >> 1)][8t + 2c + (e & 1)], position 16 * row + col.
+  // The best coordinate is the largest key
+  //   (|y| with the low 9 bits cleared) << 0 | (255 - position) << 1 | sign,
+  // one u32 maximum per lane and one warp reduction (redux.sync) per item:
+  // magnitudes order as their bits, equal truncated magnitudes go to the
+  // smaller position, and the sign bit never decides (positions differ).
+  // Truncating 9 of 23 mantissa bits (relative 2^-14) stays far below the
+  // FP16 operand rounding of the rotation itself (2^-11 per round).
+  // Positions >= D take key 0, which every position < D beats (for D < 256
+  // its position bits are >= 1 there).
+  constexpr uint32_t kMagMask = 0x7FFFFE00u;
+  const uint32_t pbase = 255u - (uint32_t)(16 * g + 2 * c);
+  const uint32_t rlim = 256u - (uint32_t)D;  // 255 - position < rlim <=> position >= D
+  uint32_t key[NI];
 #pragma unroll
   for (int i = 0; i < NI; ++i) {
-    bv[i] = -1.0f;
-    by[i] = 0.0f;
-    bp[i] = 0x7fffffff;
+    key[i] = 0u;
 #pragma unroll
     for (int t = 0; t < 2; ++t)
 #pragma unroll
       for (int e = 0; e < 4; ++e) {
-        const int pos = 16 * (g + 8 * (e >> 1)) + 8 * t + 2 * c + (e & 1);
-        const float yv = y[i][t][e];
-        const float v = yv >= 0.0f ? yv : -yv;
-        if (pos < D && (v > bv[i] || (v == bv[i] && pos < bp[i]))) {
-          bv[i] = v;
-          bp[i] = pos;
-          by[i] = yv;
-        }
+        const uint32_t u = __float_as_uint(y[i][t][e]);
+        const uint32_t rp = pbase - (uint32_t)(128 * (e >> 1) + 8 * t + (e & 1));  // 255 - position
+        uint32_t kk = (u & kMagMask) | (rp << 1) | (u >> 31);
+        if (rp < rlim) kk = 0u;
+        key[i] = max(key[i], kk);
       }
   }
 #pragma unroll
-  for (int o = 16; o; o >>= 1)
-#pragma unroll
-    for (int i = 0; i < NI; ++i) {
-      const float ov = __shfl_xor_sync(0xffffffffu, bv[i], o);
-      const int op = __shfl_xor_sync(0xffffffffu, bp[i], o);
-      const float oy = __shfl_xor_sync(0xffffffffu, by[i], o);
-      if (ov > bv[i] || (ov == bv[i] && op < bp[i])) {
-        bv[i] = ov;
-        bp[i] = op;
-        by[i] = oy;
-      }
-    }
-#pragma unroll
   for (int i = 0; i < NI; ++i) {
-    best_v[i] = bv[i];
-    best_code[i] = by[i] >= 0.0f ? bp[i] : (bp[i] | (1 << log2D));
+    const uint32_t kb = __reduce_max_sync(0xffffffffu, key[i]);
+    const int pos = 255 - (int)((kb >> 1) & 255u);
+    const uint32_t mag = kb & kMagMask;
+    best_v[i] = __uint_as_float(mag);
+    // sgn(): -0 counts as positive (FP16-product sums are 0 or >= 2^-24 in magnitude)
+    best_code[i] = ((kb & 1u) && mag) ? (pos | (1 << log2D)) : pos;
   }
 }
 
