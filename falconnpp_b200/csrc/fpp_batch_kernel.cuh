@@ -483,7 +483,7 @@ __global__ void __launch_bounds__(kBThreads, MODE == kRowsF32 ? 2 : 3) k_batch_q
         long long tot;
         const long long ex = block_exclusive_scan((long long)sz, tmp, &tot) + run;
         if (p < Qp) {
-          s_po[p] = o;
+          s_po[p] = o - (uint32_t)ex;  // candidate i of probe p is ids[i + s_po[p]] (mod 2^32)
           s_pe[p] = (uint32_t)(ex + sz);
         }
         run += tot;
@@ -501,31 +501,36 @@ __global__ void __launch_bounds__(kBThreads, MODE == kRowsF32 ? 2 : 3) k_batch_q
       const uint32_t per = (((C + kBWarps - 1) / kBWarps) + (kGStep - 1)) & ~(kGStep - 1);
       const uint32_t c_begin = min(C, (uint32_t)warp * per);
       const uint32_t c_end = min(C, c_begin + per);
-      int cur = 0;
+      // the probe of the lane's next candidate, the end of that probe's
+      // candidates and its id offset, kept in registers: a lane's candidate
+      // positions only rise, so it advances past a probe boundary (one
+      // shared-memory read) only where its candidates cross one
+      int lp = 0;
       {
         int lo = 0, hi = Qp - 1;
         while (lo < hi) {
           const int mid = (lo + hi) >> 1;
           if (s_pe[mid] > c_begin) hi = mid; else lo = mid + 1;
         }
-        cur = lo;
+        lp = lo;
       }
+      uint32_t lend = s_pe[lp], loff = s_po[lp];
       // ids of the next step are loaded while this step is inserted
       uint32_t nxt_id[kGPerLane];
       auto load_ids = [&](uint32_t c0, uint32_t (&dst)[kGPerLane]) {
-        int p = cur;  // probes rise with h
 #pragma unroll
         for (int h = 0; h < kGPerLane; ++h) {
           const uint32_t i = c0 + h * 32 + lane;
           dst[h] = kEmpty;
           if (i < c_end) {
-            while (s_pe[p] <= i) ++p;
-            const uint32_t st = p > 0 ? s_pe[p - 1] : 0u;
-            dst[h] = (uint32_t)__ldg(a.ids + s_po[p] + (i - st));
+            while (i >= lend) {  // ends when i < C = s_pe[Qp - 1]
+              ++lp;
+              lend = s_pe[lp];
+              loff = s_po[lp];
+            }
+            dst[h] = (uint32_t)__ldg(a.ids + (i + loff));
           }
         }
-        const uint32_t nx = min(c0 + kGStep, c_end > 0 ? c_end - 1 : 0u);
-        while (cur < Qp - 1 && s_pe[cur] <= nx) ++cur;
       };
       if (c_begin < c_end) load_ids(c_begin, nxt_id);
       for (uint32_t c0 = c_begin; c0 < c_end; c0 += kGStep) {
@@ -543,24 +548,35 @@ __global__ void __launch_bounds__(kBThreads, MODE == kRowsF32 ? 2 : 3) k_batch_q
             fresh[h] = id != kEmpty && (atomicOr(bits + (id >> 5), bit) & bit) == 0u;
           }
         } else {
-          // linear probing: every first probe is issued before any collision
-          // is followed.  At most kHTLimit - 1 + kBWarps * kGStep ids are ever
-          // in the table (each warp finishes at most one step after the count
-          // reaches the limit), so an empty slot always exists.
+          // linear probing in rounds: every id of the step issues its probe
+          // of the round before any result is examined, so the lane waits
+          // for the longest chain rather than for the sum of its chains.  At
+          // most kHTLimit - 1 + kBWarps * kGStep ids are ever in the table
+          // (each warp finishes at most one step after the count reaches the
+          // limit), so an empty slot always exists.
           uint32_t slot[kGPerLane], old[kGPerLane];
+          bool pend = false;
 #pragma unroll
           for (int h = 0; h < kGPerLane; ++h) {
             slot[h] = ht_slot(idv[h]);
             old[h] = idv[h] != kEmpty ? atomicCAS(sm.ht + slot[h], kEmpty, idv[h]) : kEmpty;  // no id: done
           }
 #pragma unroll
-          for (int h = 0; h < kGPerLane; ++h) {
-            while (old[h] != kEmpty && old[h] != idv[h]) {
-              slot[h] = (slot[h] + 1) & (kHT - 1);
-              old[h] = atomicCAS(sm.ht + slot[h], kEmpty, idv[h]);
+          for (int h = 0; h < kGPerLane; ++h) pend |= old[h] != kEmpty && old[h] != idv[h];
+          while (pend) {
+            pend = false;
+#pragma unroll
+            for (int h = 0; h < kGPerLane; ++h) {
+              if (old[h] != kEmpty && old[h] != idv[h]) {
+                slot[h] = (slot[h] + 1) & (kHT - 1);
+                old[h] = atomicCAS(sm.ht + slot[h], kEmpty, idv[h]);
+              }
             }
-            fresh[h] = idv[h] != kEmpty && old[h] == kEmpty;
+#pragma unroll
+            for (int h = 0; h < kGPerLane; ++h) pend |= old[h] != kEmpty && old[h] != idv[h];
           }
+#pragma unroll
+          for (int h = 0; h < kGPerLane; ++h) fresh[h] = idv[h] != kEmpty && old[h] == kEmpty;
         }
         // one position reservation per warp step
         unsigned bal[kGPerLane];
