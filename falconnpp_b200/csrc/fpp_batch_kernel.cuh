@@ -420,18 +420,25 @@ __global__ void __launch_bounds__(kBThreads, MODE == kRowsF32 ? 2 : 3) k_batch_q
     // ---- 2. global top-qProbes of the L*m lists (FalconnPP.cpp:540-582):
     // rank by counting; a tie straddling the cut replays the reference's heap
     {
+      // the order keys of the scores, once, in the top-k region (free until
+      // the replay below, which runs after the counting), padded with key 0
+      // to a multiple of 4 (scores are >= 0, so their keys exceed 0)
+      uint32_t* s_key = reinterpret_cast<uint32_t*>(s_top);
+      const int M4 = (M + 3) >> 2;
+      for (int i = tid; i < 4 * M4; i += kBThreads) s_key[i] = i < M ? ord_key(s_lv[i]) : 0u;
+      __syncthreads();
       long long run = 0;
       bool tie = false;
       for (int base = 0; base < M; base += kBThreads) {
         const int i = base + tid;
         bool take = false;
         if (i < M) {
-          const uint32_t ki = ord_key(s_lv[i]);
+          const uint32_t ki = s_key[i];
           int gt = 0, eq = 0;
-          for (int j = 0; j < M; ++j) {
-            const uint32_t kj = ord_key(s_lv[j]);
-            gt += kj > ki;
-            eq += kj == ki;
+          for (int j = 0; j < M4; ++j) {
+            const uint4 k4 = reinterpret_cast<const uint4*>(s_key)[j];
+            gt += (k4.x > ki) + (k4.y > ki) + (k4.z > ki) + (k4.w > ki);
+            eq += (k4.x == ki) + (k4.y == ki) + (k4.z == ki) + (k4.w == ki);
           }
           take = gt < Qp;
           tie |= take && gt + eq > Qp;
