@@ -540,8 +540,11 @@ __global__ void __launch_bounds__(kBThreads, MODE == kRowsF32 ? 2 : 3) k_batch_q
         }
       };
       if (c_begin < c_end) load_ids(c_begin, nxt_id);
+      // the hash set's fill as this warp last saw it: the total that its own
+      // position reservation returned (no extra shared-memory reads per step)
+      bool full = false;
       for (uint32_t c0 = c_begin; c0 < c_end; c0 += kGStep) {
-        if (!use_bitset && *(volatile unsigned*)&s_ovf) break;
+        if (full) break;
         uint32_t idv[kGPerLane];
 #pragma unroll
         for (int h = 0; h < kGPerLane; ++h) idv[h] = nxt_id[h];
@@ -559,8 +562,9 @@ __global__ void __launch_bounds__(kBThreads, MODE == kRowsF32 ? 2 : 3) k_batch_q
           // of the round before any result is examined, so the lane waits
           // for the longest chain rather than for the sum of its chains.  At
           // most kHTLimit - 1 + kBWarps * kGStep ids are ever in the table
-          // (each warp finishes at most one step after the count reaches the
-          // limit), so an empty slot always exists.
+          // (a warp inserts at most one step after its reservation shows the
+          // count at the limit; a warp with no new ids adds nothing), so an
+          // empty slot always exists.
           uint32_t slot[kGPerLane], old[kGPerLane];
           bool pend = false;
 #pragma unroll
@@ -597,6 +601,13 @@ __global__ void __launch_bounds__(kBThreads, MODE == kRowsF32 ? 2 : 3) k_batch_q
           unsigned base = 0;
           if (lane == 0) base = atomicAdd(&s_u, nfresh);
           base = __shfl_sync(kFullMask, base, 0);
+          // the warp whose reservation reaches the limit raises the flag; a
+          // warp stops after the step in which its reservation shows the
+          // limit reached, so it inserts at most one step past it
+          if (!use_bitset && base + nfresh >= kHTLimit) {
+            full = true;
+            if (lane == 0) s_ovf = 1u;
+          }
           const unsigned below = (1u << lane) - 1u;
 #pragma unroll
           for (int h = 0; h < kGPerLane; ++h) {
@@ -605,7 +616,6 @@ __global__ void __launch_bounds__(kBThreads, MODE == kRowsF32 ? 2 : 3) k_batch_q
             base += __popc(bal[h]);
           }
         }
-        if (!use_bitset && lane == 0 && *(volatile unsigned*)&s_u >= kHTLimit) s_ovf = 1u;
       }
       __syncthreads();
       if (use_bitset || !s_ovf) break;

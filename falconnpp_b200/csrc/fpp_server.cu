@@ -117,6 +117,30 @@ void finish_slot(fpp_server* S, Slot& s, int status) {
   s.nq = 0;
 }
 
+// the batch request of slot s for nq staged queries (per-query k and qProbes
+// in dK / dP)
+fpp::BatchRequest slot_request(const fpp_server* S, const Slot& s, int nq) {
+  const fpp_index* h = S->h;
+  fpp::BatchRequest rq;
+  rq.Q = s.dQ;
+  rq.nq = nq;
+  rq.q_k = s.dK;
+  rq.q_qprobes = s.dP;
+  rq.k_uniform = S->k_max;
+  rq.qprobes_uniform = S->qprobes_max;
+  rq.k_max = S->k_max;
+  rq.qprobes_max = S->qprobes_max;
+  rq.mode = h->precision;
+  rq.shortlist_mult = h->shortlist_mult;
+  rq.out = s.dOut;
+  rq.out_stride = S->k_max;
+  rq.check_status = false;
+  rq.blocks_per_sm = std::max(1, 3 / (int)S->slots.size());
+  rq.reorder = h->reorder;
+  rq.tc_rotation = h->tc_rotation;
+  return rq;
+}
+
 void worker_loop(fpp_server* S) {
   cudaSetDevice(S->device);
   const fpp_index* h = S->h;
@@ -164,23 +188,7 @@ void worker_loop(fpp_server* S) {
       cudaMemcpyAsync(s.dQ, s.hQ, sizeof(float) * (size_t)nq * d, cudaMemcpyHostToDevice, s.stream);
       cudaMemcpyAsync(s.dK, s.hK, sizeof(int32_t) * nq, cudaMemcpyHostToDevice, s.stream);
       cudaMemcpyAsync(s.dP, s.hP, sizeof(int32_t) * nq, cudaMemcpyHostToDevice, s.stream);
-      fpp::BatchRequest rq;
-      rq.Q = s.dQ;
-      rq.nq = nq;
-      rq.q_k = s.dK;
-      rq.q_qprobes = s.dP;
-      rq.k_uniform = S->k_max;
-      rq.qprobes_uniform = S->qprobes_max;
-      rq.k_max = S->k_max;
-      rq.qprobes_max = S->qprobes_max;
-      rq.mode = h->precision;
-      rq.shortlist_mult = h->shortlist_mult;
-      rq.out = s.dOut;
-      rq.out_stride = S->k_max;
-      rq.check_status = false;
-      rq.blocks_per_sm = std::max(1, 3 / (int)S->slots.size());
-      rq.reorder = h->reorder;
-      rq.tc_rotation = h->tc_rotation;
+      const fpp::BatchRequest rq = slot_request(S, s, nq);
       fpp::BatchResult res;
       fpp::Error err{0, ""};
       const int rc = fpp::batch_query(h->P, const_cast<fpp::DeviceIndex&>(h->di), s.bw, rq, s.stream, res, err);
@@ -252,6 +260,37 @@ int fpp_server_create(fpp_index* h, int n_streams, long long memory_budget_bytes
     for (Slot& s : S->slots) free_slot(s);
     delete S;
     return fpp::set_last_error(FPP_ERR_OUT_OF_MEMORY, "server_create: cannot allocate the slots");
+  }
+  // Warm-up: one batch of max_batch zero queries at k_max and qprobes_max
+  // per slot sizes the slot's batch workspace (per-block scratch, query-order
+  // buffers) for the largest batch a request mix can form, and loads the
+  // kernel.  Without it the first batches allocate while others run, and a
+  // workspace that grows frees its old buffers, which waits for the whole
+  // device: the requests in flight on every stream would see the stall.
+  for (Slot& s : S->slots) {
+    for (int i = 0; i < max_batch; ++i) {
+      s.hK[i] = k_max;
+      s.hP[i] = qprobes_max;
+    }
+    ok = ok && cudaMemsetAsync(s.dQ, 0, sizeof(float) * (size_t)max_batch * d, s.stream) == cudaSuccess;
+    ok = ok && cudaMemcpyAsync(s.dK, s.hK, sizeof(int32_t) * max_batch, cudaMemcpyHostToDevice, s.stream) == cudaSuccess;
+    ok = ok && cudaMemcpyAsync(s.dP, s.hP, sizeof(int32_t) * max_batch, cudaMemcpyHostToDevice, s.stream) == cudaSuccess;
+    if (!ok) break;
+    const fpp::BatchRequest rq = slot_request(S, s, max_batch);
+    fpp::BatchResult res;
+    fpp::Error err{0, ""};
+    const int rc = fpp::batch_query(h->P, h->di, s.bw, rq, s.stream, res, err);
+    if (rc != FPP_OK || cudaStreamSynchronize(s.stream) != cudaSuccess) {
+      for (Slot& t : S->slots) free_slot(t);
+      delete S;
+      return fpp::set_last_error(rc != FPP_OK ? rc : FPP_ERR_CUDA,
+                                 std::string("server_create: warm-up batch: ") + err.msg);
+    }
+  }
+  if (!ok) {
+    for (Slot& s : S->slots) free_slot(s);
+    delete S;
+    return fpp::set_last_error(FPP_ERR_CUDA, "server_create: warm-up staging failed");
   }
   S->worker = std::thread(worker_loop, S);
   *out = S;

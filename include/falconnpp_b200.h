@@ -186,7 +186,9 @@ int fpp_autotune(fpp_index* h, const float* d_queries, int n_queries, int k, dou
  * long as the queries and results in flight stay within
  * memory_budget_bytes (a request is always admitted into an empty slot).
  * Uses the handle's precision and shortlist setting at creation; do not
- * rebuild or clear the index while a server exists.  queries / out are host
+ * rebuild or clear the index while a server exists.  Creation runs one
+ * batch of max_batch zero queries per stream, which sizes each stream's
+ * workspace for the largest batch, so serving allocates nothing.  queries / out are host
  * buffers that must stay valid until fpp_server_wait returns for the ticket;
  * wait on each ticket exactly once.  latency_ms: submit to results written. */
 typedef struct fpp_server fpp_server;

@@ -155,3 +155,26 @@ def test_tensor_core_rotation(precision):
             assert val[qi, j] == np.float32(oracle.dot(Q[qi], Xc[ids[qi, j]]))
     # the same batch again gives the same ids (the rotation is deterministic)
     assert np.array_equal(_batched(g, Q, 20, 10, precision=precision, mult=4), ids)
+
+
+@pytest.mark.parametrize("precision", [0, 2])
+def test_hash_set_overflow_falls_back_to_bitset(precision):
+    # few, large buckets: a query's probes reach far more than the 5,120
+    # unique ids the shared-memory hash set takes, so the batched kernel
+    # restarts that query's gather on its L2 bitset; FP32 must still equal
+    # the plain path bit for bit, and every form must be deterministic
+    # (about two thirds of these queries pass the limit, so one batch runs
+    # both dedupe paths)
+    X = synth.mixture(40000, 64, n_centres=2, seed=0)
+    Q = synth.mixture(64, 64, n_centres=2, seed=1)
+    g = _index(X, 4, 64, 8000, 0.5, 2)
+    g.set_qprobes(32)
+    plain = g.query(Q, 10)
+    st = g.stats(1)
+    assert st[1] / len(Q) > 5120, st[1]  # unique candidates per query, on average past the limit
+    got = _batched(g, Q, 10, 32, precision=precision, mult=4)
+    if precision == 0:
+        assert np.array_equal(got, plain)
+    else:
+        assert synth.recall_at_k(plain, got, 10) >= 0.9
+    assert np.array_equal(_batched(g, Q, 10, 32, precision=precision, mult=4), got)
