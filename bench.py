@@ -55,6 +55,15 @@ FORM_SPECS = {
 FORMS = ["plain-fp32", "batched-fp32", "batched-bf16", "batched-fp8"]
 RECALL_SAMPLE = 500
 RECALL_TARGET = 0.90
+METRIC = "QPS @ recall@20>=0.9, batched BF16/FP8 vs plain FP32 (1M x 200 MIPS); p99 ms per 10k-query batch"
+
+
+def workload_config(args, w, qprobes):
+    """The workload half of the JSON line's config, the same on both arms."""
+    return {"workload": args.workload, "n_points": w["n"], "d": w["d"], "n_tables": w["L"], "n_proj": w["D"],
+            "iProbes": w["iProbes"], "bucket_minSize": w["minSize"], "bucket_scale": w["alpha"],
+            "queries_per_step": w["nq"], "k": w["k"], "qProbes": qprobes,
+            "l2": "inputs larger than L2 (126 MB)"}
 
 
 def log(*a):
@@ -305,7 +314,7 @@ def run_ours(args, w, rank, world, local_rank):
         traffic = traffic * U if traffic else None
 
     result = {
-        "metric": "QPS @ recall@20>=0.9, batched BF16/FP8 vs plain FP32 (1M x 200 MIPS); p99 ms per 10k-query batch",
+        "metric": METRIC,
         "value": round(hr["value"], 1),
         "unit": "queries/s",
         "n_gpus": world,
@@ -317,10 +326,7 @@ def run_ours(args, w, rank, world, local_rank):
         "vs_baseline": None,
         "dtype": {0: "f32", 1: "bf16 rerank, f32 hash/re-score", 2: "fp8-e4m3 rerank, f32 hash/re-score"}[prec],
         "data": "synthetic",
-        "config": {"workload": args.workload, "n_points": n, "d": d, "n_tables": w["L"], "n_proj": w["D"],
-                   "iProbes": w["iProbes"], "bucket_minSize": w["minSize"], "bucket_scale": w["alpha"],
-                   "queries_per_step": nq, "k": k, "qProbes": chosen, "form": head,
-                   "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (index 1.9 GB)"},
+        "config": dict(workload_config(args, w, chosen), form=head, parallelism=f"replicas{world}"),
         "recall_at_k": round(hr["recall"], 4),
         "recall_sweep_plain": sweep_log,
         "forms": {f: {"value": round(v["value"], 1), "ms_per_step": round(v["ms"], 4), "recall_at_k": round(v["recall"], 4)}
@@ -392,7 +398,7 @@ def run_reference(args, w):
     total = sum(ts)
     value = nsamp * args.steps / total
     return {
-        "metric": "QPS @ recall@20>=0.9 (1M x 200 MIPS, plain FP32 form); p99 ms per 10k-query batch",
+        "metric": METRIC,
         "impl": "reference",
         "value": round(value, 1),
         "unit": "queries/s",
@@ -405,12 +411,11 @@ def run_reference(args, w):
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic",
-        "config": {"workload": args.workload, "n_points": w["n"], "d": w["d"], "n_tables": w["L"],
-                   "n_proj": w["D"], "iProbes": w["iProbes"], "qProbes": qp, "k": w["k"],
-                   "queries_per_step": nsamp, "form": "reference CPU path (oracle port, OpenMP)"},
+        "config": dict(workload_config(args, w, qp), form="reference CPU path (oracle port, OpenMP)",
+                       parallelism=f"host-threads{threads}"),
         "build_s": round(build_s, 2),
         "cpu_baseline": {"value": round(value, 1), "unit": "queries/s", "cores": threads, "kind": "port",
-                         "sample": f"{nsamp} queries per step of the 10k-query batch"},
+                         "sample": f"{nsamp} of the batch's {w['nq']} queries per step"},
         "e2e": {"value": round(value, 1), "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 
@@ -694,7 +699,7 @@ def main():
         import torch
         import torch.distributed as dist
         torch.cuda.set_device(local_rank)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=180))
     res = run_ours(args, w, rank, world, local_rank)
     if world > 1:
         import torch.distributed as dist
