@@ -653,6 +653,19 @@ __global__ void __launch_bounds__(kBThreads, MODE == kRowsF32 ? 2 : 3) k_batch_q
     if (MODE == kRowsF32) {
       rerank_rows<MODE, VI, 2>(uq, U, sc, sm.q, a.Xrows, a.row_bytes, a.nchunk, nullptr, warp, kBWarps, lane,
                                s_hist);
+    } else if (a.nchunk <= 16 && 9 * 16 * a.row_bytes <= (size_t)(4 * kHT) &&
+               7 * 16 * a.row_bytes <= BatchSmem<GROUPS>::kQ - BatchSmem<GROUPS>::kProbe) {
+      // two tiles in flight per warp, both staged in shared memory that the
+      // rerank leaves idle: the hash-set region (reset at the end of the
+      // query) holds every warp's first stage and warp 7's second, the
+      // probe list, top-k and rotation regions (unused until the shortlist)
+      // the second stages of warps 0..6
+      const size_t sb = 16 * a.row_bytes;
+      unsigned char* st0 = smem_raw + (size_t)warp * sb;
+      unsigned char* st1 = warp < kBWarps - 1 ? smem_raw + BatchSmem<GROUPS>::kProbe + (size_t)warp * sb
+                                              : smem_raw + (size_t)kBWarps * sb;
+      rerank_rows_mma_2stage<MODE>(uq, U, sc, sm.qx, a.Xrows, a.row_bytes, a.nchunk, a.Xscale, qscale, warp,
+                                   kBWarps, lane, s_hist, st0, st1);
     } else {
       rerank_rows_mma<MODE>(uq, U, sc, sm.qx, a.Xrows, a.row_bytes, a.nchunk, a.Xscale, qscale, warp, kBWarps,
                             lane, s_hist);

@@ -347,4 +347,147 @@ __device__ __forceinline__ void rerank_rows_mma(const uint32_t* ids, unsigned U,
   }
 }
 
+// 16-byte cp.async from global memory into shared memory (cached in L2
+// only), a 16-byte shared-memory load, and group control of the calling
+// thread's outstanding copies
+__device__ __forceinline__ void cp_async16(uint32_t saddr, const void* gmem) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(saddr), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ uint4 ld_shared_u4(uint32_t saddr) {
+  uint4 v;
+  asm volatile("ld.shared.v4.u32 {%0,%1,%2,%3}, [%4];\n"
+               : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+               : "r"(saddr)
+               : "memory");
+  return v;
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_one() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// rerank_rows_mma with two tiles in flight per warp, both in shared memory:
+// the warp's tiles alternate between two stages of 16 * row_bytes bytes
+// (stage0, stage1), filled by cp.async and read back with 16-byte shared
+// loads right before the mma, so no registers hold rows in flight.  Rows
+// of one load round only (nchunk <= 16).  Each lane copies and later reads
+// back only its own chunks (4j + c of rows g and g + 8), so waiting for its
+// own copy groups suffices; a stage is refilled only after the mma that
+// consume its chunks have been issued.  The products and their order are
+// those of rerank_rows_mma, so the scores are the same bits.  Returns with
+// no copy in flight.
+template <int MODE>
+__device__ __forceinline__ void rerank_rows_mma_2stage(const uint32_t* ids, unsigned U, uint32_t* score,
+                                                       const unsigned char* qx, const unsigned char* rows,
+                                                       size_t row_bytes, int nchunk, const float* scale, float qscale,
+                                                       int warp, int nwarps, int lane, uint32_t* hist11,
+                                                       unsigned char* stage0, unsigned char* stage1) {
+  using P = QueryParts<MODE>;
+  const int g = lane >> 2;
+  const int c = lane & 3;
+  const unsigned ntiles = (U + 15u) >> 4;
+  const unsigned nw = (unsigned)nwarps;
+  const int JN = (nchunk + 3) >> 2;  // chunk rounds of 4 (<= 4 here)
+  const uint4* qpart = reinterpret_cast<const uint4*>(qx) + (g < P::NP ? g : 0) * P::PC + c;
+  const uint4 zero = make_uint4(0u, 0u, 0u, 0u);
+  // shared address of the lane's chunk c of row g in each stage; row g + 8
+  // is 8 rows further
+  const uint32_t lane_off = (uint32_t)(g * row_bytes) + 16u * (uint32_t)c;
+  const uint32_t sa0 = (uint32_t)__cvta_generic_to_shared(stage0) + lane_off;
+  const uint32_t sa1 = (uint32_t)__cvta_generic_to_shared(stage1) + lane_off;
+  const uint32_t rb8 = 8u * (uint32_t)row_bytes;
+  auto tile_ids = [&](unsigned t, uint32_t& i0, uint32_t& i1) {
+    i0 = i1 = kNoRow;
+    if (t < ntiles) {
+      const unsigned r0 = t * 16u + g;
+      if (r0 < U) i0 = ids[r0];
+      if (r0 + 8u < U) i1 = ids[r0 + 8u];
+    }
+  };
+  // start copying the rows i0, i1 into the stage at sa (one commit group,
+  // empty when both are absent); the FP8 row scales load at the same time
+  auto issue = [&](uint32_t sa, uint32_t i0, uint32_t i1, float& f0, float& f1) {
+    const unsigned char* p0 = rows + (size_t)(i0 != kNoRow ? i0 : 0u) * row_bytes + 16u * (unsigned)c;
+    const unsigned char* p1 = rows + (size_t)(i1 != kNoRow ? i1 : 0u) * row_bytes + 16u * (unsigned)c;
+#pragma unroll
+    for (int jj = 0; jj < 4; ++jj) {
+      if (4 * jj + c < nchunk) {
+        if (i0 != kNoRow) cp_async16(sa + 64u * jj, p0 + 64 * jj);
+        if (i1 != kNoRow) cp_async16(sa + rb8 + 64u * jj, p1 + 64 * jj);
+      }
+    }
+    cp_async_commit();
+    f0 = f1 = 1.0f;
+    if (MODE == kRowsFP8 && c == 0) {
+      f0 = i0 != kNoRow ? __ldg(scale + i0) : 0.0f;
+      f1 = i1 != kNoRow ? __ldg(scale + i1) : 0.0f;
+    }
+  };
+  // the tile held in the stage at sa: mma over its chunks, then the scores
+  // (row g: columns 2c, 2c+1 in acc[0..1]; row g + 8 in acc[2..3])
+  auto compute = [&](unsigned t, uint32_t sa, uint32_t i0, uint32_t i1, float f0, float f1) {
+    float acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll
+    for (int jj = 0; jj < 4; ++jj) {
+      if (jj < JN) {
+        const bool ok = 4 * jj + c < nchunk;
+        const uint4 a0 = (ok && i0 != kNoRow) ? ld_shared_u4(sa + 64u * jj) : zero;
+        const uint4 a1 = (ok && i1 != kNoRow) ? ld_shared_u4(sa + rb8 + 64u * jj) : zero;
+        const uint4 b = g < P::NP ? qpart[4 * jj] : zero;
+        if (MODE == kRowsBF16) {
+          mma_bf16_m16n8k16(acc, a0.x, a1.x, a0.y, a1.y, b.x, b.y);
+          mma_bf16_m16n8k16(acc, a0.z, a1.z, a0.w, a1.w, b.z, b.w);
+        } else {
+          mma_e4m3_m16n8k32(acc, a0.x, a1.x, a0.y, a1.y, b.x, b.y);
+          mma_e4m3_m16n8k32(acc, a0.z, a1.z, a0.w, a1.w, b.z, b.w);
+        }
+      }
+    }
+    const unsigned r0 = t * 16u + g;
+    const unsigned r1 = r0 + 8u;
+    float s0 = acc[0] + acc[1];
+    float s1 = acc[2] + acc[3];
+    s0 += __shfl_xor_sync(0xffffffffu, s0, 1);
+    s1 += __shfl_xor_sync(0xffffffffu, s1, 1);
+    s0 += __shfl_xor_sync(0xffffffffu, s0, 2);
+    s1 += __shfl_xor_sync(0xffffffffu, s1, 2);
+    if (c == 0) {
+      if (r0 < U) {
+        const float v = MODE == kRowsFP8 ? s0 * qscale * f0 : s0;
+        score[r0] = __float_as_uint(v);
+        if (hist11) atomicAdd(hist11 + (ord_key_bits(__float_as_uint(v)) >> 21), 1u);
+      }
+      if (r1 < U) {
+        const float v = MODE == kRowsFP8 ? s1 * qscale * f1 : s1;
+        score[r1] = __float_as_uint(v);
+        if (hist11) atomicAdd(hist11 + (ord_key_bits(__float_as_uint(v)) >> 21), 1u);
+      }
+    }
+  };
+  unsigned t = (unsigned)warp;
+  uint32_t a0, a1, b0, b1, na0, na1, nb0, nb1;
+  float fa0, fa1, fb0, fb1;
+  // two commit groups always in order: stage 0's, then stage 1's
+  tile_ids(t, a0, a1);
+  tile_ids(t + nw, b0, b1);
+  issue(sa0, a0, a1, fa0, fa1);
+  issue(sa1, b0, b1, fb0, fb1);
+  tile_ids(t + 2u * nw, na0, na1);
+  tile_ids(t + 3u * nw, nb0, nb1);
+  for (; t < ntiles; t += 2u * nw) {
+    cp_async_wait_one();  // stage 0's group (the older one) has landed
+    compute(t, sa0, a0, a1, fa0, fa1);
+    a0 = na0;
+    a1 = na1;
+    issue(sa0, a0, a1, fa0, fa1);  // tile t + 2 nw (its mma above were issued first)
+    cp_async_wait_one();  // stage 1's group has landed
+    if (t + nw < ntiles) compute(t + nw, sa1, b0, b1, fb0, fb1);
+    b0 = nb0;
+    b1 = nb1;
+    issue(sa1, b0, b1, fb0, fb1);  // tile t + 3 nw
+    tile_ids(t + 4u * nw, na0, na1);
+    tile_ids(t + 5u * nw, nb0, nb1);
+  }
+  cp_async_wait_all();
+}
+
 }  // namespace fpp
