@@ -21,7 +21,7 @@ EXPORTED = [
     "fpp_dump_tables", "fpp_build_dump_hash", "fpp_query_dump", "fpp_rerank_probes_noalloc",
     "fpp_set_query_form", "fpp_query_batched", "fpp_autotune",
     "fpp_server_create", "fpp_server_submit", "fpp_server_wait", "fpp_server_stats", "fpp_server_destroy",
-    "fpp_bruteforce_topk_f64",
+    "fpp_bruteforce_topk_f64", "fpp_save", "fpp_load", "fpp_load_txt", "fpp_output_file",
 ]
 
 _lib = None
@@ -71,6 +71,10 @@ def lib() -> ctypes.CDLL:
             "fpp_server_stats": (i32, [vp, vp, i32]),
             "fpp_server_destroy": (None, [vp]),
             "fpp_bruteforce_topk_f64": (i32, [vp, i64, i32, vp, i32, i32, vp, vp, vp]),
+            "fpp_save": (i32, [vp, ctypes.c_char_p]),
+            "fpp_load": (i32, [vp, ctypes.c_char_p]),
+            "fpp_load_txt": (i32, [ctypes.c_char_p, i32, i32, vp, vp]),
+            "fpp_output_file": (i32, [ctypes.c_char_p, vp, i32, i32]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -176,10 +180,10 @@ class Index:
                     agreement=rep[4], tried=int(rep[5]))
 
     def info(self) -> dict:
-        v = np.zeros(6, np.int64)
-        _check(lib().fpp_get_info(self.h, _ptr(v), 6))
+        v = np.zeros(9, np.int64)
+        _check(lib().fpp_get_info(self.h, _ptr(v), 9))
         return dict(fhtDim=int(v[0]), n_ids=int(v[1]), max_kept=int(v[2]), n_buckets=int(v[3]), built=bool(v[4]),
-                    device=int(v[5]))
+                    device=int(v[5]), n_tables=int(v[6]), n_proj=int(v[7]), iProbes=int(v[8]))
 
     def stats(self, kind: int) -> np.ndarray:
         v = np.zeros(10, np.float64)
@@ -188,7 +192,7 @@ class Index:
 
     def dump_bits(self):
         info = self.info()
-        nbits = self.L * 3 * info["fhtDim"]
+        nbits = info["n_tables"] * 3 * info["fhtDim"]
         b1 = np.zeros(nbits, np.uint8)
         b2 = np.zeros(nbits, np.uint8)
         _check(lib().fpp_dump_bits(self.h, _ptr(b1), _ptr(b2)))
@@ -198,6 +202,12 @@ class Index:
         c = np.zeros(self.d, np.float32)
         _check(lib().fpp_dump_center(self.h, _ptr(c)))
         return c
+
+    def save(self, path: str):
+        _check(lib().fpp_save(self.h, os.fsencode(path)))
+
+    def load(self, path: str):
+        _check(lib().fpp_load(self.h, os.fsencode(path)))
 
     def dump_tables(self):
         info = self.info()
@@ -256,3 +266,19 @@ def bruteforce_topk_f64(x_ptr: int, n: int, d: int, q_ptr: int, nq: int, k: int,
     _check(lib().fpp_bruteforce_topk_f64(ctypes.c_void_p(x_ptr), n, d, ctypes.c_void_p(q_ptr), nq, k,
                                          ctypes.c_void_p(out_ptr), ctypes.c_void_p(val_ptr or 0),
                                          ctypes.c_void_p(stream or 0)))
+
+
+def load_txt(path: str, n_points: int, n_features: int):
+    """The reference's loadtxtData (src/Utilities.cpp:42-61): n_points lines of
+    n_features floats.  Returns (X, n_read): X is (n_points, n_features)
+    float32, zero where the file runs short."""
+    X = np.zeros((n_points, n_features), np.float32)
+    got = ctypes.c_longlong(0)
+    _check(lib().fpp_load_txt(os.fsencode(path), n_points, n_features, _ptr(X), ctypes.addressof(got)))
+    return X, got.value
+
+
+def output_file(path: str, topk: np.ndarray) -> None:
+    """The reference's outputFile (src/Utilities.cpp:13-33): one query per line."""
+    t = np.ascontiguousarray(topk, dtype=np.int32)
+    _check(lib().fpp_output_file(os.fsencode(path), _ptr(t), t.shape[0], t.shape[1]))

@@ -553,6 +553,47 @@ void free_index(DeviceIndex& di) {
   di = DeviceIndex();
 }
 
+int upload_flips(const Params& P, const HostBits& bits, DeviceIndex& di, cudaStream_t s, Error& err) {
+  const int L = P.n_tables, F = P.fhtDim;
+  const int WORDS = F < 32 ? 1 : F / 32;
+  std::vector<uint32_t> hflips((size_t)2 * L * 3 * WORDS, 0u);
+  std::vector<uint32_t> htflips;
+  for (int layer = 0; layer < 2; ++layer) {
+    const std::vector<uint8_t>& b = layer == 0 ? bits.b1 : bits.b2;
+    for (int l = 0; l < L; ++l)
+      for (int r = 0; r < 3; ++r)
+        for (int i = 0; i < F; ++i) {
+          const uint8_t bit = b[(size_t)l * 3 * F + (size_t)r * F + i];
+          if (bit == 0) hflips[(((size_t)layer * L + l) * 3 + r) * WORDS + i / 32] |= 1u << (i % 32);
+        }
+  }
+  FPP_CUDA(cudaMalloc(&di.flips, sizeof(uint32_t) * hflips.size()));
+  FPP_CUDA(cudaMemcpyAsync(di.flips, hflips.data(), sizeof(uint32_t) * hflips.size(), cudaMemcpyHostToDevice, s));
+  if (F == 256) {
+    // the tensor-core rotation (batched low-precision form) reads round 2's
+    // signs in the transposed view: bit 16k + n of its words is the sign of
+    // position 16n + k
+    htflips = hflips;
+    for (size_t v = 0; v < (size_t)2 * L; ++v) {
+      const uint32_t* src = hflips.data() + (v * 3 + 1) * WORDS;
+      uint32_t* dst = htflips.data() + (v * 3 + 1) * WORDS;
+      for (int w = 0; w < WORDS; ++w) dst[w] = 0u;
+      for (int pp = 0; pp < 256; ++pp) {
+        const int p0 = 16 * (pp & 15) + (pp >> 4);
+        if ((src[p0 >> 5] >> (p0 & 31)) & 1u) dst[pp >> 5] |= 1u << (pp & 31);
+      }
+    }
+    FPP_CUDA(cudaMalloc(&di.tflips, sizeof(uint32_t) * htflips.size()));
+    FPP_CUDA(cudaMemcpyAsync(di.tflips, htflips.data(), sizeof(uint32_t) * htflips.size(), cudaMemcpyHostToDevice,
+                             s));
+  }
+  // the host vectors go out of scope here
+  FPP_CUDA(cudaStreamSynchronize(s));
+  return kOk;
+fail:
+  return err.code;
+}
+
 int build_index(const Params& P, const float* X, bool x_on_device, const HostBits& bits,
                 const BuildOptions& opt, DeviceIndex& di, BuildStats& st, cudaStream_t s, Error& err,
                 int32_t* dump_codes, float* dump_scores) {
@@ -560,7 +601,6 @@ int build_index(const Params& P, const float* X, bool x_on_device, const HostBit
   const long long n = P.n_points;
   const int d = P.n_features, L = P.n_tables, D = P.n_proj, F = P.fhtDim, IP = P.iProbes;
   const uint32_t NB = 4u * (uint32_t)D * (uint32_t)D;
-  const int WORDS = F < 32 ? 1 : F / 32;
   const int ld = (d + 3) & ~3;
   int log2D = 0;
   while ((1 << log2D) < D) ++log2D;
@@ -590,7 +630,6 @@ int build_index(const Params& P, const float* X, bool x_on_device, const HostBit
   uint64_t ids_capacity = 0;
   int h_bad = 0;
   unsigned long long h_base = 0;
-  std::vector<uint32_t> hflips, htflips;
   long long tables_per_chunk = 0;
   const long long entry_cap = 1LL << 27;
   long long max_entries = 0;
@@ -634,36 +673,7 @@ int build_index(const Params& P, const float* X, bool x_on_device, const HostBit
   }
 
   // 2. random signs -> flip words [2][L][3][WORDS]
-  hflips.assign((size_t)2 * L * 3 * WORDS, 0u);
-  for (int layer = 0; layer < 2; ++layer) {
-    const std::vector<uint8_t>& b = layer == 0 ? bits.b1 : bits.b2;
-    for (int l = 0; l < L; ++l)
-      for (int r = 0; r < 3; ++r)
-        for (int i = 0; i < F; ++i) {
-          const uint8_t bit = b[(size_t)l * 3 * F + (size_t)r * F + i];
-          if (bit == 0) hflips[(((size_t)layer * L + l) * 3 + r) * WORDS + i / 32] |= 1u << (i % 32);
-        }
-  }
-  FPP_CUDA(cudaMalloc(&di.flips, sizeof(uint32_t) * hflips.size()));
-  FPP_CUDA(cudaMemcpyAsync(di.flips, hflips.data(), sizeof(uint32_t) * hflips.size(), cudaMemcpyHostToDevice, s));
-  if (F == 256) {
-    // the tensor-core rotation (batched low-precision form) reads round 2's
-    // signs in the transposed view: bit 16k + n of its words is the sign of
-    // position 16n + k
-    htflips = hflips;
-    for (size_t v = 0; v < (size_t)2 * L; ++v) {
-      const uint32_t* src = hflips.data() + (v * 3 + 1) * WORDS;
-      uint32_t* dst = htflips.data() + (v * 3 + 1) * WORDS;
-      for (int w = 0; w < WORDS; ++w) dst[w] = 0u;
-      for (int pp = 0; pp < 256; ++pp) {
-        const int p0 = 16 * (pp & 15) + (pp >> 4);
-        if ((src[p0 >> 5] >> (p0 & 31)) & 1u) dst[pp >> 5] |= 1u << (pp & 31);
-      }
-    }
-    FPP_CUDA(cudaMalloc(&di.tflips, sizeof(uint32_t) * htflips.size()));
-    FPP_CUDA(cudaMemcpyAsync(di.tflips, htflips.data(), sizeof(uint32_t) * htflips.size(), cudaMemcpyHostToDevice,
-                             s));
-  }
+  if (upload_flips(P, bits, di, s, err) != kOk) goto fail;
 
   // 3. hash + sort + compact, a chunk of tables at a time
   tables_per_chunk = opt.tables_per_chunk > 0 ? opt.tables_per_chunk

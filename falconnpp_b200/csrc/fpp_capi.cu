@@ -631,13 +631,16 @@ int fpp_query_dump(fpp_index* h, const float* queries, int n_queries, int n_neig
 int fpp_get_info(fpp_index* h, long long* out, int n) {
   if (!h || !out) return fail(FPP_ERR_INVALID_ARGUMENT, "get_info: NULL argument");
   std::lock_guard<std::mutex> g(h->mu);
-  const long long v[6] = {h->P.fhtDim,
+  const long long v[9] = {h->P.fhtDim,
                           (long long)h->di.n_ids,
                           (long long)h->di.max_kept,
                           (long long)h->P.n_tables * 4LL * h->P.n_proj * h->P.n_proj,
                           h->built ? 1LL : 0LL,
-                          h->device};
-  for (int i = 0; i < n && i < 6; ++i) out[i] = v[i];
+                          h->device,
+                          h->P.n_tables,
+                          h->P.n_proj,
+                          h->P.iProbes};
+  for (int i = 0; i < n && i < 9; ++i) out[i] = v[i];
   return ok();
 }
 

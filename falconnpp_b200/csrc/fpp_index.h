@@ -87,6 +87,11 @@ int build_index(const Params& P, const float* X, bool x_on_device, const HostBit
 
 void free_index(DeviceIndex& di);
 
+// The sign flip words (and, for fhtDim 256, their per-view copy for the
+// tensor-core rotation) from the sign bits, into di.flips / di.tflips;
+// synchronises s before returning.
+int upload_flips(const Params& P, const HostBits& bits, DeviceIndex& di, cudaStream_t s, Error& err);
+
 int derived_fht_dim(int n_features, int n_proj);
 
 }  // namespace fpp

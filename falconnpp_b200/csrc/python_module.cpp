@@ -68,6 +68,14 @@ class FalconnPP {
     return out;
   }
 
+  // additions (no reference counterpart): persist a built index, and load
+  // one saved for the same n_points x n_features
+  void save(const std::string& path) { check(fpp_save(h_, path.c_str())); }
+  void load(const std::string& path) {
+    py::gil_scoped_release nogil;
+    check(fpp_load(h_, path.c_str()));
+  }
+
   fpp_index* handle() const { return h_; }
 
  private:
@@ -89,5 +97,25 @@ PYBIND11_MODULE(FalconnPP, m) {
       .def("build2D", &FalconnPP::build, py::arg("dataset"))
       .def("query2D", &FalconnPP::query, py::arg("queries"), py::arg("n_neighbors"), py::arg("verbose") = false)
       .def("build", &FalconnPP::build, py::arg("dataset"))
-      .def("query", &FalconnPP::query, py::arg("queries"), py::arg("n_neighbors"), py::arg("verbose") = false);
+      .def("query", &FalconnPP::query, py::arg("queries"), py::arg("n_neighbors"), py::arg("verbose") = false)
+      .def("save", &FalconnPP::save, py::arg("path"))
+      .def("load", &FalconnPP::load, py::arg("path"));
+  // the reference's text formats (src/Utilities.cpp:13-61): loadtxtData
+  // returns the (n_features, n_points) matrix build() takes; outputFile
+  // writes a (Q, k) top-k array one query per line
+  m.def(
+      "loadtxtData",
+      [](const std::string& path, int n_points, int n_features) {
+        py::array_t<float, py::array::f_style> X({(py::ssize_t)n_features, (py::ssize_t)n_points});
+        check(fpp_load_txt(path.c_str(), n_points, n_features, X.mutable_data(), nullptr));
+        return X;
+      },
+      py::arg("dataset"), py::arg("numPoints"), py::arg("numDim"));
+  m.def(
+      "outputFile",
+      [](const py::array_t<int32_t, py::array::c_style | py::array::forcecast>& topk, const std::string& path) {
+        if (topk.ndim() != 2) throw py::value_error("outputFile: top-k must be a (Q, k) int32 array");
+        check(fpp_output_file(path.c_str(), topk.data(), (int)topk.shape(0), (int)topk.shape(1)));
+      },
+      py::arg("matKNN"), py::arg("outputFile"));
 }

@@ -85,7 +85,8 @@ int fpp_query_device(fpp_index* h, const float* d_queries, int n_queries, int n_
 const char* fpp_last_error(void);
 
 /* Index facts: out[0] fhtDim, out[1] stored ids, out[2] largest stored bucket,
- * out[3] buckets (n_tables * 4 * n_proj^2), out[4] built (0/1), out[5] device. */
+ * out[3] buckets (n_tables * 4 * n_proj^2), out[4] built (0/1), out[5] device,
+ * out[6] n_tables, out[7] n_proj, out[8] iProbes (the first n are written). */
 int fpp_get_info(fpp_index* h, long long* out, int n);
 
 /* Statistics of the last build (kind 0) or query (kind 1) as doubles.
@@ -211,6 +212,32 @@ void fpp_server_destroy(fpp_server* s);
  * written. */
 int fpp_bruteforce_topk_f64(const float* d_X, long long n_points, int n_features, const float* d_Q, int n_queries,
                             int k, int32_t* d_out, double* d_out_val, void* stream);
+
+/* Index persistence (no counterpart in the reference, which rebuilds its
+ * index on every run): fpp_save writes a built index (parameters, sign bits,
+ * centre, centred rows, CSR bucket offsets and ids) to one binary file;
+ * fpp_load reads it into a handle created for the same n_points x
+ * n_features, which is then built (setIndexParam is not needed).  fpp_load
+ * checks the header, the file size, the sign bits, the offsets (from 0,
+ * non-decreasing, ending at the id count) and every id (in [0, n_points))
+ * before the handle uses them; a rejected file leaves the handle's previous
+ * index untouched if the header or sign bits fail, and the handle unbuilt if
+ * a later section fails.  Query results after a load equal those of the
+ * index that was saved. */
+int fpp_save(fpp_index* h, const char* path);
+int fpp_load(fpp_index* h, const char* path);
+
+/* The reference's text matrix formats (src/Utilities.cpp:13-61), for the
+ * command-line workflow.  fpp_load_txt reads n_points lines of n_features
+ * whitespace-separated floats into out (n_points x n_features, one point per
+ * row: the d x n column-major matrix of loadtxtData); like the reference it
+ * leaves 0 where the file runs short, and *n_read (may be NULL) reports how
+ * many values it read; a missing file is an error (the reference exits).
+ * fpp_output_file writes topk (n_queries x k int32) one query per line, each
+ * id followed by a space, as outputFile does for the K x Q matrix the
+ * reference's query returns. */
+int fpp_load_txt(const char* path, int n_points, int n_features, float* out, long long* n_read);
+int fpp_output_file(const char* path, const int32_t* topk, int n_queries, int k);
 
 /* No counterpart in the reference.  The gather, deduplicate, rerank and top-k
  * stage of fpp_query for callers that cannot allocate device memory: code
