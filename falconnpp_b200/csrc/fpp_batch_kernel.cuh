@@ -242,6 +242,11 @@ constexpr size_t batch_smem_bytes() {
 }
 
 __device__ __forceinline__ uint32_t ht_slot(uint32_t id) { return (id * 2654435761u) >> (32 - 13); }
+// the probe stride of an id (double hashing): odd, so with the power-of-two
+// table every slot is reached, and from an independent multiplier, so ids
+// that share a first slot take different paths (linear probing's clusters
+// made a 256-id step wait for chains of ~11 probes at 55 % fill)
+__device__ __forceinline__ uint32_t ht_step(uint32_t id) { return ((id * 0x85EBCA6Bu) >> (32 - 13)) | 1u; }
 
 // HASH: kHashAuto rotates on the tensor cores where a query keeps one probe
 // per table (and a.tflips is set), exactly otherwise; kHashTC only on the
@@ -558,7 +563,7 @@ __global__ void __launch_bounds__(kBThreads, MODE == kRowsF32 ? 2 : 3) k_batch_q
             fresh[h] = id != kEmpty && (atomicOr(bits + (id >> 5), bit) & bit) == 0u;
           }
         } else {
-          // linear probing in rounds: every id of the step issues its probe
+          // open addressing (double hashing) in rounds: every id of the step issues its probe
           // of the round before any result is examined, so the lane waits
           // for the longest chain rather than for the sum of its chains.  At
           // most kHTLimit - 1 + kBWarps * kGStep ids are ever in the table
@@ -579,7 +584,7 @@ __global__ void __launch_bounds__(kBThreads, MODE == kRowsF32 ? 2 : 3) k_batch_q
 #pragma unroll
             for (int h = 0; h < kGPerLane; ++h) {
               if (old[h] != kEmpty && old[h] != idv[h]) {
-                slot[h] = (slot[h] + 1) & (kHT - 1);
+                slot[h] = (slot[h] + ht_step(idv[h])) & (kHT - 1);
                 old[h] = atomicCAS(sm.ht + slot[h], kEmpty, idv[h]);
               }
             }
