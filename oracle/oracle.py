@@ -1,9 +1,14 @@
-"""ctypes wrapper of the CPU oracle (oracle/falconnpp_oracle.cpp).
+"""ctypes wrappers of the CPU checkers: the oracle (oracle/falconnpp_oracle.cpp,
+a restatement of the reference's algorithm) and the reference's own code
+compiled from its sources (oracle/_ref/libfalconnpp_ref.so: src/FalconnPP.cpp,
+src/Utilities.cpp and src/fht.c unchanged, against the Eigen / Boost subset in
+oracle/shim/, through oracle/ref_harness.cpp).
 
 TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
-CPU-baseline leg of bench.py, never by the product.  ``build()`` compiles the
-oracle (and, when the reference tree is present, the reference's own fht.c
-into oracle/_ref/) with the Makefile beside this file.
+CPU legs of bench.py, never by the product.  ``build()`` compiles the oracle
+and, when the reference tree is present, the oracle/_ref libraries, with the
+Makefile beside this file.  The reference tree is taken from the environment
+variable FPP_REFERENCE_ROOT when it is set, else the Makefile's default.
 """
 from __future__ import annotations
 
@@ -16,16 +21,25 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "_build", "liboracle.so")
 REF_FHT = os.path.join(HERE, "_ref", "libfht_ref.so")
+REF_LIB = os.path.join(HERE, "_ref", "libfalconnpp_ref.so")
 
 _lib = None
+_ref_lib = None
+
+
+def _make_args() -> list[str]:
+    root = os.environ.get("FPP_REFERENCE_ROOT")
+    return [f"REF={root}"] if root else []
 
 
 def build(force: bool = False) -> None:
+    """Compile the oracle, and the oracle/_ref libraries where the reference
+    tree is present (make decides from the sources' timestamps)."""
     if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < os.path.getmtime(
             os.path.join(HERE, "falconnpp_oracle.cpp")):
-        subprocess.run(["make", "-C", HERE, "-B" if force else "-s"], check=True, capture_output=True)
-    elif os.path.isdir("/root/reference") and not os.path.exists(REF_FHT):
-        subprocess.run(["make", "-C", HERE, "ref"], check=True, capture_output=True)
+        subprocess.run(["make", "-C", HERE, "-B" if force else "-s", "_build/liboracle.so" if not force else "all",
+                        *_make_args()], check=True, capture_output=True)
+    subprocess.run(["make", "-C", HERE, "-s", "ref", *_make_args()], check=True, capture_output=True)
 
 
 def lib() -> ctypes.CDLL:
@@ -202,3 +216,127 @@ class Index:
         out = np.zeros(cap, np.int32)
         c = int(lib().orc_query_candidates(self.h, _p(q), _p(out), cap))
         return out[:c]
+
+
+def ref_lib() -> ctypes.CDLL | None:
+    """The reference's own FalconnPP code (compiled from its sources), if built."""
+    global _ref_lib
+    if _ref_lib is None:
+        if not os.path.exists(REF_LIB):
+            return None
+        L = ctypes.CDLL(REF_LIB)
+        vp, i32, i64, f32 = ctypes.c_void_p, ctypes.c_int, ctypes.c_longlong, ctypes.c_float
+        sig = {
+            "ref_create": (vp, [i32, i32]),
+            "ref_destroy": (None, [vp]),
+            "ref_set_index_param": (None, [vp, i32, i32, i32, f32, i32, i32, i32]),
+            "ref_set_qprobes": (None, [vp, i32]),
+            "ref_set_threads": (None, [vp, i32]),
+            "ref_build": (None, [vp, vp, i32]),
+            "ref_query": (None, [vp, vp, i32, i32, i32, i32, vp]),
+            "ref_import": (None, [vp, vp, vp, vp, i64, vp, i64, vp, i64]),
+            "ref_fht_dim": (i32, [vp]),
+            "ref_num_ids": (i64, [vp]),
+            "ref_num_buckets": (i64, [vp]),
+            "ref_get_tables": (None, [vp, vp, vp, vp]),
+            "ref_num_ids_2d": (i64, [vp]),
+            "ref_get_tables_2d": (None, [vp, vp, vp]),
+            "ref_get_centered": (None, [vp, vp]),
+            "ref_get_bits": (None, [vp, vp, vp]),
+        }
+        for name, (res, args) in sig.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _ref_lib = L
+    return _ref_lib
+
+
+class Reference:
+    """The reference's FalconnPP class itself (src/FalconnPP.h:10-132), built
+    from its own sources: setIndexParam / build / set_qProbes / query, and
+    the 2D build2D / query2D, plus reads of its index internals."""
+
+    def __init__(self, n: int, d: int):
+        L = ref_lib()
+        if L is None:
+            raise RuntimeError("oracle/_ref/libfalconnpp_ref.so is not built (the reference tree is absent)")
+        self.n, self.d = n, d
+        self.h = L.ref_create(n, d)
+        self.two_d = False
+
+    def __del__(self):
+        try:
+            ref_lib().ref_destroy(self.h)
+        except Exception:
+            pass
+
+    def set_index_param(self, L, D, minSize, alpha, iProbes, threads=0, seed=-1):
+        ref_lib().ref_set_index_param(self.h, L, D, minSize, alpha, iProbes, threads, seed)
+        self.L, self.D, self.iProbes = L, D, iProbes
+        self.fht = int(ref_lib().ref_fht_dim(self.h))
+
+    def set_qprobes(self, q):
+        self.qProbes = q
+        ref_lib().ref_set_qprobes(self.h, q)
+
+    def set_threads(self, t):
+        ref_lib().ref_set_threads(self.h, t)
+
+    def build(self, X: np.ndarray, two_d: bool = False):
+        self._X = np.ascontiguousarray(X, np.float32)
+        self.two_d = two_d
+        ref_lib().ref_build(self.h, _p(self._X), int(two_d))
+
+    def query(self, Q: np.ndarray, k: int, verbose: bool = False) -> np.ndarray:
+        Q = np.ascontiguousarray(Q, np.float32)
+        out = np.zeros((Q.shape[0], k), np.int32)
+        ref_lib().ref_query(self.h, _p(Q), Q.shape[0], k, int(verbose), int(self.two_d), _p(out))
+        return out
+
+    def bits(self):
+        nbits = self.L * 3 * self.fht
+        b1 = np.zeros(nbits, np.uint8)
+        b2 = np.zeros(nbits, np.uint8)
+        ref_lib().ref_get_bits(self.h, _p(b1), _p(b2))
+        return b1, b2
+
+    def import_index(self, Xc, b1, b2, start, ids):
+        """Adopt an index built elsewhere (dumped from the GPU): its queries
+        then run through the reference's own query2Layers_1D."""
+        Xc = np.ascontiguousarray(Xc, np.float32)
+        b1 = np.ascontiguousarray(b1, np.uint8)
+        b2 = np.ascontiguousarray(b2, np.uint8)
+        start = np.ascontiguousarray(start, np.uint32)
+        ids = np.ascontiguousarray(ids, np.int32)
+        if np.diff(start.astype(np.int64)).max(initial=0) > 65535:
+            raise ValueError("a bucket holds more than 65535 ids (the reference's uint16 size)")
+        ref_lib().ref_import(self.h, _p(Xc), _p(b1), _p(b2), b1.size, _p(start), start.size - 1, _p(ids), ids.size)
+        self.two_d = False
+
+    def centered(self) -> np.ndarray:
+        Xc = np.zeros((self.n, self.d), np.float32)
+        ref_lib().ref_get_centered(self.h, _p(Xc))
+        return Xc
+
+    def buckets(self):
+        """Per bucket (global id l * 4D^2 + h): the reference's ids in its
+        stored order.  Returns (sizes, ids concatenated in bucket order)."""
+        L = ref_lib()
+        if self.two_d:
+            nb = self.L * 4 * self.D * self.D
+            size = np.zeros(nb, np.uint32)
+            ids = np.zeros(max(1, int(L.ref_num_ids_2d(self.h))), np.int32)
+            L.ref_get_tables_2d(self.h, _p(size), _p(ids))
+            return size.astype(np.int64), ids[: int(size.sum())]
+        nb = int(L.ref_num_buckets(self.h))
+        pos = np.zeros(nb, np.uint32)
+        size = np.zeros(nb, np.uint16)
+        raw = np.zeros(max(1, int(L.ref_num_ids(self.h))), np.int32)
+        L.ref_get_tables(self.h, _p(pos), _p(size), _p(raw))
+        size = size.astype(np.int64)
+        # gather each bucket's range [pos, pos + size) into bucket order
+        total = int(size.sum())
+        starts = np.repeat(pos.astype(np.int64), size)
+        within = np.arange(total, dtype=np.int64) - np.repeat(np.cumsum(size) - size, size)
+        return size, raw[starts + within]
