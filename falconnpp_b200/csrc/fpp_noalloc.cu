@@ -2,23 +2,31 @@
 // rerank / top-k stage of a query for callers that cannot allocate device
 // memory.
 //
-// Who needs it: code that runs where cudaMalloc is off limits — inside a CUDA
-// stream capture being recorded into a graph by someone else, in a serving
+// Who needs it: code that runs where cudaMalloc is off limits — a serving
 // thread with a hard latency budget (cudaMalloc and cudaFree synchronise the
-// device and can stall for milliseconds), or in a host process whose device
-// memory is owned by another allocator.  fpp_query allocates its workspace on
-// first use and grows it with the batch; this entry point allocates nothing.
+// device and can stall for milliseconds), or a host process whose device
+// memory is owned by another allocator (a framework's caching pool, a
+// pre-sized arena) that must not see foreign allocations.  fpp_query
+// allocates its workspace on first use and grows it with the batch; this
+// entry point allocates nothing.  The call waits for its kernel (it reads a
+// status word back), so it is a blocking call on its stream.
 //
 // How: the per-block scratch the stage needs (a dedupe bitset of n bits, the
 // unique-candidate list and its scores) lives in one file-scope __device__
 // array of kScratchBytes (64 MiB).  Every GPU that loads the library holds that
 // array until the process exits.  Host code cannot use the array's name as a
 // device address, so the first call on each device looks the address up with
-// cudaGetSymbolAddress (with that device current) and caches it; make that
-// first call before any stream capture.  Every call shares the one array and
-// keeps the previous call's contents, so each call clears the bitsets and the
-// status word before its kernel runs; two calls whose kernels overlap on the
-// GPU (two streams, or two handles on one device) race on it.
+// cudaGetSymbolAddress (with that device current) and caches it.  Every call
+// shares the one array and keeps the previous call's contents, so each call
+// clears the status word and the bitsets of the blocks it uses before its
+// kernel runs (the unique lists and scores are written before they are read);
+// two calls whose kernels overlap on the GPU (two streams, or two handles on
+// one device) race on it.
+//
+// The probes come from the caller, so every probe id is checked against the
+// index's bucket count on the device: an id outside [0, n_tables * 4 *
+// n_proj^2) reads nothing, sets a status bit, and the call returns
+// FPP_ERR_INVALID_ARGUMENT.
 //
 // The results are those of fpp_query for the same probes: same canonical FP32
 // dot order, same top-k with the exact heap replay on ties
@@ -56,6 +64,7 @@ __host__ __device__ inline size_t align256(size_t x) { return (x + 255) & ~size_
 
 struct NoAllocArgs {
   const uint32_t* probes;
+  uint32_t nbuckets;  // n_tables * 4 * n_proj^2: valid probe ids are below it
   int nq, qProbes, k;
   const uint32_t* bucket_off;
   const int32_t* ids;
@@ -118,9 +127,15 @@ __global__ void __launch_bounds__(kThreads) k_gather_rerank_noalloc(NoAllocArgs 
       const int np = min(kProbeChunk, a.qProbes - p0);
       for (int i = tid; i < np; i += kThreads) {
         const uint32_t g = pr[p0 + i];
-        const uint32_t o = a.bucket_off[g];
+        uint32_t o = 0, sz = 0;
+        if (g < a.nbuckets) {
+          o = a.bucket_off[g];
+          sz = a.bucket_off[g + 1] - o;
+        } else {
+          atomicOr(status, 2u);  // a probe id outside the index: read nothing
+        }
         s_po[i] = o;
-        s_ps[i] = a.bucket_off[g + 1] - o;
+        s_ps[i] = sz;
       }
       __syncthreads();
       for (int p = warp; p < np; p += kWarps) {
@@ -338,11 +353,14 @@ extern "C" int fpp_rerank_probes_noalloc(fpp_index* h, const float* d_queries, i
   }
   const size_t block_bytes = bitset_bytes + 2 * align256((size_t)cap * 4);
   cudaStream_t s = stream ? (cudaStream_t)stream : h->stream;
-  // what must start at zero: the status word and the bitsets of the blocks used
-  e = cudaMemsetAsync(scratch, 0, kStatusBytes + (size_t)grid * block_bytes, s);
+  // what must start at zero: the status word and the bitsets of the blocks
+  // used (one row of bitset_bytes at the start of each block's region)
+  e = cudaMemsetAsync(scratch, 0, kStatusBytes, s);
+  if (e == cudaSuccess) e = cudaMemset2DAsync(scratch + kStatusBytes, block_bytes, 0, bitset_bytes, (size_t)grid, s);
   if (e != cudaSuccess) return set_last_error(FPP_ERR_CUDA, std::string("rerank_noalloc: memset: ") + cudaGetErrorString(e));
   NoAllocArgs a;
   a.probes = d_probes;
+  a.nbuckets = (uint32_t)((long long)h->P.n_tables * 4LL * h->P.n_proj * h->P.n_proj);
   a.nq = n_queries;
   a.qProbes = n_probes;
   a.k = n_neighbors;
@@ -364,6 +382,10 @@ extern "C" int fpp_rerank_probes_noalloc(fpp_index* h, const float* d_queries, i
   e = cudaMemcpyAsync(&status, scratch, sizeof(status), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return set_last_error(FPP_ERR_CUDA, std::string("rerank_noalloc: ") + cudaGetErrorString(e));
+  if (status & 2u)
+    return set_last_error(FPP_ERR_INVALID_ARGUMENT,
+                          "rerank_noalloc: a probe id is outside [0, n_tables * 4 * n_proj^2); it was read as an "
+                          "empty bucket");
   if (status)
     return set_last_error(FPP_ERR_UNSUPPORTED,
                           "rerank_noalloc: a query has more unique candidates than the scratch holds per block "

@@ -1,6 +1,8 @@
 """fpp_rerank_probes_noalloc: the allocation-free variant of the gather /
-rerank / top-k stage, for callers that cannot call cudaMalloc (graph
-recording, latency-critical serving threads, foreign allocators).
+rerank / top-k stage, for callers that cannot call cudaMalloc
+(latency-critical serving threads, whose cudaMalloc / cudaFree would
+synchronise the device, and processes whose device memory belongs to another
+allocator).
 
 It is called through the C ABI with device buffers the test owns, twice in a
 row (the second call sees the scratch the first one left behind), and must
@@ -62,4 +64,45 @@ def test_noalloc_rejects_bad_sizes():
                                               2, 2000, ctypes.c_void_p(out.data_ptr()), None)
     assert rc == capi.FPP_ERR_INVALID_ARGUMENT
     assert b"n_neighbors" in capi.lib().fpp_last_error()
+    g.close()
+
+
+def test_noalloc_rejects_out_of_range_probe():
+    # caller-supplied probes are checked on the device: an id past the
+    # index's n_tables * 4 * n_proj^2 buckets is read as an empty bucket and
+    # the call reports it; the other queries' rows are still those of the
+    # same probes without the bad id
+    import torch
+
+    n, d, k, qprobes = 5000, 32, 5, 4
+    X = synth.mixture(n, d, n_centres=8, seed=0)
+    Q = synth.mixture(16, d, n_centres=8, seed=1)
+    g = capi.Index(n, d)
+    g.set_index_param(4, 32, 10, 0.05, 2, 8, 3)
+    g.build(X)
+    g.set_qprobes(qprobes)
+    ref = g.query_dump(Q, k, qprobes)
+    probes = ref["probes"].copy()
+    nb = g.info()["n_buckets"]
+    probes[3, 1] = nb  # one past the last bucket
+    probes[7, 0] = 0xFFFFFFF0
+    dq = torch.from_numpy(Q).cuda()
+    dp = torch.from_numpy(probes.view(np.int32)).cuda()
+    out = torch.full((Q.shape[0], k), -7, dtype=torch.int32, device="cuda")
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    rc = capi.lib().fpp_rerank_probes_noalloc(g.h, ctypes.c_void_p(dq.data_ptr()), Q.shape[0],
+                                              ctypes.c_void_p(dp.data_ptr()), qprobes, k,
+                                              ctypes.c_void_p(out.data_ptr()), stream)
+    assert rc == capi.FPP_ERR_INVALID_ARGUMENT
+    assert b"probe id" in capi.lib().fpp_last_error()
+    got = out.cpu().numpy()
+    good = [i for i in range(Q.shape[0]) if i not in (3, 7)]
+    assert np.array_equal(got[good], ref["topk"][good])
+    # the next call with valid probes succeeds (the status word is cleared)
+    dp = torch.from_numpy(ref["probes"].view(np.int32)).cuda()
+    rc = capi.lib().fpp_rerank_probes_noalloc(g.h, ctypes.c_void_p(dq.data_ptr()), Q.shape[0],
+                                              ctypes.c_void_p(dp.data_ptr()), qprobes, k,
+                                              ctypes.c_void_p(out.data_ptr()), stream)
+    assert rc == 0, capi.lib().fpp_last_error().decode()
+    assert np.array_equal(out.cpu().numpy(), ref["topk"])
     g.close()
