@@ -48,6 +48,18 @@ def _newer(target: str, deps: list[str]) -> bool:
     return all(os.path.getmtime(d) <= t for d in deps)
 
 
+FLAGS_FILE = os.path.join(HERE, "_build", "build_flags.json")
+LINK_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-shared"]
+
+
+def _record_flags() -> None:
+    """The flags the library's objects and link were made with (read by the
+    tests to check the target architecture without inspecting the binary)."""
+    import json
+    with open(FLAGS_FILE, "w") as f:
+        json.dump({"compile": NVCC_FLAGS, "link": LINK_FLAGS, "sources": CU_SOURCES}, f, indent=1)
+
+
 def build_library(force: bool = False) -> str:
     objdir = os.path.join(HERE, "_build")
     os.makedirs(objdir, exist_ok=True)
@@ -65,8 +77,10 @@ def build_library(force: bool = False) -> str:
     with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
         list(ex.map(_run, jobs))
     if force or jobs or not _newer(LIB, objs):
-        _run([_nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", LIB, *objs,
-              "-Xlinker", "--no-undefined"])
+        _run([_nvcc(), *LINK_FLAGS, "-o", LIB, *objs, "-Xlinker", "--no-undefined"])
+        _record_flags()
+    elif not os.path.exists(FLAGS_FILE):
+        _record_flags()
     return LIB
 
 

@@ -19,7 +19,7 @@ EXPORTED = [
     "fpp_build", "fpp_build_device", "fpp_query", "fpp_query_device", "fpp_last_error", "fpp_get_info",
     "fpp_get_stats", "fpp_set_option", "fpp_print_build_report", "fpp_dump_bits", "fpp_dump_center",
     "fpp_dump_tables", "fpp_build_dump_hash", "fpp_query_dump", "fpp_rerank_probes_noalloc",
-    "fpp_set_query_form", "fpp_query_batched", "fpp_autotune",
+    "fpp_set_query_form", "fpp_query_batched", "fpp_query_batched_dump", "fpp_autotune",
     "fpp_server_create", "fpp_server_submit", "fpp_server_wait", "fpp_server_stats", "fpp_server_destroy",
     "fpp_bruteforce_topk_f64", "fpp_save", "fpp_load", "fpp_load_txt", "fpp_output_file",
 ]
@@ -64,6 +64,7 @@ def lib() -> ctypes.CDLL:
             "fpp_rerank_probes_noalloc": (i32, [vp, vp, i32, vp, i32, i32, vp, vp]),
             "fpp_set_query_form": (i32, [vp, i32, i32, i32]),
             "fpp_query_batched": (i32, [vp, vp, i32, vp, vp, i32, i32, vp, i32, vp, vp]),
+            "fpp_query_batched_dump": (i32, [vp, vp, i32, i32, vp, vp, vp, vp, vp]),
             "fpp_autotune": (i32, [vp, vp, i32, i32, ctypes.c_double, vp, vp]),
             "fpp_server_create": (i32, [vp, i32, i64, i32, i32, i32, ctypes.POINTER(vp)]),
             "fpp_server_submit": (i32, [vp, vp, i32, i32, i32, vp, ctypes.POINTER(i64)]),
@@ -171,6 +172,12 @@ class Index:
         _check(lib().fpp_query_batched(self.h, ctypes.c_void_p(q_ptr), nq, ctypes.c_void_p(k_ptr or 0),
                                        ctypes.c_void_p(qp_ptr or 0), k_max, qp_max, ctypes.c_void_p(out_ptr),
                                        out_stride, ctypes.c_void_p(val_ptr or 0), ctypes.c_void_p(stream or 0)))
+
+    def query_batched_dump(self, q_ptr: int, nq: int, k: int, out_ptr: int, val_ptr: int | None,
+                           probes_ptr: int | None, counts_ptr: int | None, stream: int | None = None):
+        _check(lib().fpp_query_batched_dump(self.h, ctypes.c_void_p(q_ptr), nq, k, ctypes.c_void_p(out_ptr),
+                                            ctypes.c_void_p(val_ptr or 0), ctypes.c_void_p(probes_ptr or 0),
+                                            ctypes.c_void_p(counts_ptr or 0), ctypes.c_void_p(stream or 0)))
 
     def autotune(self, q_ptr: int, nq: int, k: int, min_agreement: float = 0.99, stream: int | None = None) -> dict:
         rep = np.zeros(6, np.float64)

@@ -338,9 +338,11 @@ int batch_query(const Params& P, DeviceIndex& di, BatchWorkspace& bw, const Batc
   a.status = bw.counters + 1;
   a.order = reorder ? bw.order : nullptr;
   a.tflips = (rq.tc_rotation && rq.mode != kRowsF32 && F == 256) ? di.tflips : nullptr;
+  a.dump_probes = rq.dump_probes;
+  a.dump_counts = rq.dump_counts;
   void* args[] = {&a};
 
-  const bool can_graph = rq.use_graph;
+  const bool can_graph = rq.use_graph && !rq.dump_probes && !rq.dump_counts;
   BatchKey key{rq.Q, rq.nq, rq.q_k, rq.q_qprobes, rq.k_uniform, rq.qprobes_uniform, rq.k_max, rq.qprobes_max,
                rq.shortlist_mult, rq.out,
                rq.out_stride, rq.out_v, rq.mode, grid, kern, bw.bitset, a.order, a.tflips, s};

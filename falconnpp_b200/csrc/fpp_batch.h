@@ -23,7 +23,10 @@ struct BatchRequest {
   bool check_status = true;        // synchronise and report overflow
   int blocks_per_sm = 0;           // 0 = as many as fit
   bool reorder = true;             // process the queries grouped by a locality key
-  bool tc_rotation = true;         // BF16/FP8, fhtDim 256: rotate on the tensor cores (FP16 operands)
+  uint32_t* dump_probes = nullptr;  // parity dumps (device, nullable; no graph): [nq][qprobes_max] probes
+  uint32_t* dump_counts = nullptr;  // [nq][2] candidates, unique candidates
+  bool tc_rotation = false;        // opt-in, BF16/FP8, fhtDim 256: rotate on the tensor cores (FP16 operands,
+                                   // not the reference's FP32 hash: probes can differ)
 };
 
 struct BatchResult {

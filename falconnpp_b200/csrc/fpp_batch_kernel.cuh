@@ -65,6 +65,8 @@ struct BatchArgs {
   unsigned int* status;  // bit 0: candidate capacity overflow; bit 1: per-query k/qProbes out of range
   const uint32_t* order;  // processing order of the queries (nullable: 0, 1, ...)
   const uint32_t* tflips;  // non-null: rotate on the tensor cores when a query keeps one probe per table
+  uint32_t* dump_probes;   // parity dump (nullable): [nq][qprobes_max] probed global bucket ids
+  uint32_t* dump_counts;   // parity dump (nullable): [nq][2] candidates, unique candidates
 };
 
 __device__ __forceinline__ int ceil_sqrt_int(int m) {
@@ -382,11 +384,7 @@ __global__ void __launch_bounds__(kBThreads, MODE == kRowsF32 ? 2 : 3) k_batch_q
           hd3_rotate<FHT>(y, a.flips + ((size_t)(layer * L + lt) * 3) * WORDS, gl);
           float* lv = sm.gv + (grp * 2 + layer) * (kBMaxM1 + 1);
           int* lc = sm.gc + (grp * 2 + layer) * (kBMaxM1 + 1);
-          const int f = group_top_cp_auto<FHT>(y, gl, a.D, a.log2D, cnt, lv, lc);
-          __syncwarp();
-          bool ok = (f == cnt);
-          for (int t = 1; t < cnt; ++t)
-            if (ok && !(lv[t - 1] > lv[t])) ok = false;
+          const bool ok = group_top_cp_checked<FHT>(y, gl, a.D, a.log2D, m1, cnt, lv, lc);
           if (!ok) {
 #pragma unroll
             for (int e = 0; e < E; ++e) ydump[gl * E + e] = y[e];
@@ -473,6 +471,8 @@ __global__ void __launch_bounds__(kBThreads, MODE == kRowsF32 ? 2 : 3) k_batch_q
       }
       __syncthreads();
     }
+    if (a.dump_probes)
+      for (int j = tid; j < Qp; j += kBThreads) a.dump_probes[(size_t)q * a.qprobes_max + j] = s_probe[j];
 
     // ---- 3. gather + dedupe (FalconnPP.cpp:584-606): the candidates of all
     // probes flattened over the warps; dedupe in a shared-memory hash set, or
@@ -631,6 +631,10 @@ __global__ void __launch_bounds__(kBThreads, MODE == kRowsF32 ? 2 : 3) k_batch_q
       __syncthreads();
     }
     const unsigned U = s_u;
+    if (a.dump_counts && tid == 0) {
+      a.dump_counts[2 * (size_t)q] = C;
+      a.dump_counts[2 * (size_t)q + 1] = U;
+    }
     int32_t* orow = a.out + (size_t)q * a.out_stride;
     float* ovrow = a.out_v ? a.out_v + (size_t)q * a.out_stride : nullptr;
     if (U > cap) {

@@ -589,6 +589,42 @@ int fpp_query_batched(fpp_index* h, const float* d_queries, int n_queries, const
   return ok();
 }
 
+int fpp_query_batched_dump(fpp_index* h, const float* d_queries, int n_queries, int n_neighbors, int32_t* d_out,
+                           float* d_out_val, uint32_t* d_probes, uint32_t* d_counts, void* stream) {
+  if (!h) return fail(FPP_ERR_INVALID_ARGUMENT, "query_batched_dump: NULL handle");
+  std::lock_guard<std::mutex> g(h->mu);
+  int rc = check_query_params(h, n_queries, n_neighbors);
+  if (rc) return rc;
+  if (n_queries == 0) return ok();
+  if (!d_queries || !d_out) return fail(FPP_ERR_INVALID_ARGUMENT, "query_batched_dump: NULL buffer");
+  if (use_device(h)) return FPP_ERR_CUDA;
+  cudaStream_t s = stream ? (cudaStream_t)stream : h->stream;
+  fpp::BatchRequest rq;
+  rq.Q = d_queries;
+  rq.nq = n_queries;
+  rq.k_uniform = n_neighbors;
+  rq.qprobes_uniform = h->P.qProbes;
+  rq.k_max = n_neighbors;
+  rq.qprobes_max = h->P.qProbes;
+  rq.mode = h->precision;
+  rq.shortlist_mult = h->shortlist_mult;
+  rq.out = d_out;
+  rq.out_stride = n_neighbors;
+  rq.out_v = d_out_val;
+  rq.blocks_per_sm = h->blocks_per_sm;
+  rq.reorder = h->reorder;
+  rq.tc_rotation = h->tc_rotation;
+  rq.dump_probes = d_probes;
+  rq.dump_counts = d_counts;
+  rq.check_status = true;
+  fpp::BatchResult res;
+  fpp::Error err{0, ""};
+  rc = fpp::batch_query(h->P, h->di, h->bw, rq, s, res, err);
+  if (rc) return fail(rc, err.msg);
+  if (res.overflow) return fail(FPP_ERR_UNSUPPORTED, "query_batched_dump: candidate capacity exceeded");
+  return ok();
+}
+
 int fpp_query_dump(fpp_index* h, const float* queries, int n_queries, int n_neighbors, int32_t* out,
                    float* topk_val, uint32_t* probes, float* probe_val, long long* stats, int32_t* cands,
                    long long cand_cap) {

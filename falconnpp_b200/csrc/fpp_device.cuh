@@ -33,10 +33,57 @@ struct Geo {
 __device__ __forceinline__ uint32_t ord_key(float f) { return ord_key_bits(__float_as_uint(f)); }
 
 // In-place FWHT of the group's vector, stages in increasing stride.
+//
+// With 32 elements per lane, elements j and j + 16 travel as one pair through
+// Blackwell's packed FP32 instructions (__fadd2_rn / __ffma2_rn: each
+// component rounds exactly like __fadd_rn / __fmaf_rn), so every stage except
+// h = 16 (which pairs j with j + 16 itself) issues half the instructions.
+// The difference a - b is fma(-1, b, a): the product is exact, so its single
+// rounding is that of the subtraction (zeros included).
 template <int FHT>
 __device__ __forceinline__ void fwht_group(float (&y)[Geo<FHT>::E], int gl) {
   constexpr int E = Geo<FHT>::E;
   constexpr int G = Geo<FHT>::G;
+  if constexpr (E == 32) {
+    const float2 neg = make_float2(-1.0f, -1.0f);
+#pragma unroll
+    for (int h = 1; h < 16; h <<= 1) {
+#pragma unroll
+      for (int i = 0; i < 16; i += 2 * h) {
+#pragma unroll
+        for (int j = i; j < i + h; ++j) {
+          const float2 a = make_float2(y[j], y[j + 16]);
+          const float2 b = make_float2(y[j + h], y[j + h + 16]);
+          const float2 sum = __fadd2_rn(a, b);
+          const float2 dif = __ffma2_rn(neg, b, a);
+          y[j] = sum.x;
+          y[j + 16] = sum.y;
+          y[j + h] = dif.x;
+          y[j + h + 16] = dif.y;
+        }
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+      const float a = y[j];
+      const float b = y[j + 16];
+      y[j] = __fadd_rn(a, b);
+      y[j + 16] = __fsub_rn(a, b);
+    }
+#pragma unroll
+    for (int s = 1; s < G; s <<= 1) {
+      const float sg = (gl & s) ? -1.0f : 1.0f;
+      const float2 sgn2 = make_float2(sg, sg);
+#pragma unroll
+      for (int e = 0; e < 16; ++e) {
+        const float2 o = make_float2(__shfl_xor_sync(kFullMask, y[e], s), __shfl_xor_sync(kFullMask, y[e + 16], s));
+        const float2 r = __ffma2_rn(sgn2, make_float2(y[e], y[e + 16]), o);
+        y[e] = r.x;
+        y[e + 16] = r.y;
+      }
+    }
+    return;
+  }
 #pragma unroll
   for (int h = 1; h < E; h <<= 1) {
 #pragma unroll
@@ -287,6 +334,56 @@ __device__ __forceinline__ int group_top2_cp(const float (&y)[Geo<FHT>::E], int 
   return found;
 }
 
+// The top-1 of cp_value over coordinates r < D in canonical order (lane gl
+// == 0 writes out_v[0], out_c[0]) and whether it is strict: true when no
+// other coordinate has an equal value and D >= 2.  That is exactly the
+// condition under which group_top2_cp's first two entries are in strict
+// order, so callers that keep one entry per layer (m1 = 1, iProbes = 1) use
+// it in place of the top-2 with the same tie replay.  Two passes: the group
+// maximum of |y| (one max per element), then the count, first position and
+// signed value of the elements equal to it.
+template <int FHT>
+__device__ __forceinline__ bool group_top1_strict(const float (&y)[Geo<FHT>::E], int gl, int D, int log2D,
+                                                  float* out_v, int* out_c) {
+  constexpr int E = Geo<FHT>::E;
+  constexpr int G = Geo<FHT>::G;
+  const int lim = D - gl * E;  // elements of this lane that are coordinates (< D)
+  float lm = -1.0f;
+  if (lim >= E) {
+#pragma unroll
+    for (int e = 0; e < E; ++e) lm = fmaxf(lm, fabsf(y[e]));
+  } else {
+#pragma unroll
+    for (int e = 0; e < E; ++e)
+      if (e < lim) lm = fmaxf(lm, fabsf(y[e]));
+  }
+  float gm = lm;
+#pragma unroll
+  for (int s = 1; s < G; s <<= 1) gm = fmaxf(gm, __shfl_xor_sync(kFullMask, gm, s));
+  int cnt = 0, pos = 0;
+  float sy = 0.0f;
+#pragma unroll
+  for (int e = E - 1; e >= 0; --e) {
+    const bool eq = e < lim && fabsf(y[e]) == gm;
+    cnt += eq ? 1 : 0;
+    pos = eq ? e : pos;
+    sy = eq ? y[e] : sy;
+  }
+  int tot = cnt;
+#pragma unroll
+  for (int s = 1; s < G; s <<= 1) tot += __shfl_xor_sync(kFullMask, tot, s);
+  const int base = (int)(threadIdx.x & 31) & ~(G - 1);
+  const unsigned gbits = (__ballot_sync(kFullMask, cnt > 0) >> base) & (G == 32 ? kFullMask : ((1u << G) - 1u));
+  const int owner_gl = gbits ? __ffs(gbits) - 1 : 0;
+  const float wy = __shfl_sync(kFullMask, sy, base + owner_gl);
+  const int wpos = __shfl_sync(kFullMask, pos, base + owner_gl);
+  if (gl == 0) {
+    out_v[0] = cp_value(wy);
+    out_c[0] = cp_code(wy, owner_gl * E + wpos, log2D);
+  }
+  return tot == 1 && D >= 2;
+}
+
 // Dispatch: the single-pass selection when cnt is small, the round-based one
 // otherwise.
 template <int FHT>
@@ -295,6 +392,28 @@ __device__ __forceinline__ int group_top_cp_auto(const float (&y)[Geo<FHT>::E], 
   if (cnt <= 2) return group_top2_cp<FHT>(y, gl, D, log2D, cnt, out_v, out_c);
   if (cnt <= 4) return group_top_cp_small<FHT, 4>(y, gl, D, log2D, cnt, out_v, out_c);
   return group_top_cp<FHT>(y, gl, D, log2D, cnt, out_v, out_c);
+}
+
+// Top-cnt selection with the strictness check every caller applies: true
+// when the group found cnt entries in strictly decreasing order (no tie can
+// change the kept set), false when the reference's heap scan must be
+// replayed.  keep is the number of entries the caller uses (cnt = keep + 1
+// unless D is smaller); keeping one (m1 = 1 or iProbes = 1) takes the
+// two-pass strict top-1, which writes only entry 0.
+template <int FHT>
+__device__ __forceinline__ bool group_top_cp_checked(const float (&y)[Geo<FHT>::E], int gl, int D, int log2D,
+                                                     int keep, int cnt, float* out_v, int* out_c) {
+  if (keep == 1 && cnt == 2) {
+    const bool ok = group_top1_strict<FHT>(y, gl, D, log2D, out_v, out_c);
+    __syncwarp();
+    return ok;
+  }
+  const int f = group_top_cp_auto<FHT>(y, gl, D, log2D, cnt, out_v, out_c);
+  __syncwarp();
+  bool ok = (f == cnt);
+  for (int t = 1; t < cnt; ++t)
+    if (ok && !(out_v[t - 1] > out_v[t])) ok = false;
+  return ok;
 }
 
 // Exact replay of the reference's per-layer top-p scan (FalconnPP.cpp:103-156,

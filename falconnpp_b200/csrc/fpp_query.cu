@@ -100,11 +100,7 @@ __global__ void __launch_bounds__(128, 4) k_query_hash(QHashArgs a, float* heap_
       hd3_rotate<FHT>(y, a.flips + ((size_t)(layer * a.L + l) * 3) * WORDS, gl);
       float* lv = layer == 0 ? lv1 : lv2;
       int* lc = layer == 0 ? lc1 : lc2;
-      const int f = group_top_cp_auto<FHT>(y, gl, a.D, a.log2D, cnt, lv, lc);
-      __syncwarp();
-      bool ok = (f == cnt);
-      for (int t = 1; t < cnt; ++t)
-        if (ok && !(lv[t - 1] > lv[t])) ok = false;
+      const bool ok = group_top_cp_checked<FHT>(y, gl, a.D, a.log2D, m1, cnt, lv, lc);
       if (!ok) {
 #pragma unroll
         for (int e = 0; e < E; ++e) ydump[gl * E + e] = y[e];

@@ -108,10 +108,12 @@ int fpp_get_stats(fpp_index* h, int kind, double* out, int n);
  * "reorder_queries" (default 1: the batched form processes a batch grouped by
  * the first table's first-layer bucket code, so queries in flight together
  * share buckets and rows in L2; results are unchanged), "tc_rotation"
- * (default 1: the batched BF16/FP8 form with fhtDim 256 and one probe per
- * table rotates on the tensor cores with FP16 operands and FP32 accumulation;
- * its probes can differ from the exact FP32 rotation's where two rotated
- * coordinates or two bucket scores are within about 1e-3 of each other). */
+ * (default 0, opt-in: the batched BF16/FP8 form with fhtDim 256 and one probe
+ * per table rotates on the tensor cores with FP16 operands and FP32
+ * accumulation instead of the reference's FP32 arithmetic; its probes can then
+ * differ from the reference's where two rotated coordinates or two bucket
+ * scores are within about 1e-3 of each other.  With the default, every form
+ * hashes in exact FP32 and probes the reference's buckets). */
 int fpp_set_option(fpp_index* h, const char* key, long long value);
 
 /* Prints the build report the reference writes to stdout after
@@ -150,8 +152,10 @@ int fpp_query_dump(fpp_index* h, const float* queries, int n_queries, int n_neig
  * plain path bit for bit; precision 1 (BF16) and 2 (FP8-E4M3 with a per-row
  * scale) rerank the candidates in low precision with FP32 accumulation and
  * re-score the best shortlist_mult * k of them in exact FP32.  The hashing is
- * FP32 and identical in every form.  Extends query2Layers_1D; no reference
- * counterpart for the batched form. */
+ * the reference's FP32 arithmetic in every form (unless the opt-in
+ * "tc_rotation" option is set), so every form probes the same buckets and
+ * gathers the same candidates; only the low-precision rerank differs.
+ * Extends query2Layers_1D; no reference counterpart for the batched form. */
 int fpp_set_query_form(fpp_index* h, int form, int precision, int shortlist_mult);
 
 /* Batched form with per-query k and qProbes (mixed batches).  d_k and
@@ -165,6 +169,18 @@ int fpp_set_query_form(fpp_index* h, int form, int precision, int shortlist_mult
 int fpp_query_batched(fpp_index* h, const float* d_queries, int n_queries, const int32_t* d_k,
                       const int32_t* d_qprobes, int k_max, int qprobes_max, int32_t* d_out, int out_stride,
                       float* d_out_val, void* stream);
+
+/* Parity dump of the batched form (no reference counterpart): runs the
+ * handle's batched configuration (precision, shortlist, the handle's qProbes,
+ * uniform k) on device queries and also writes, per query, the probed global
+ * bucket ids (d_probes, n_queries x qProbes, the probed set in no particular
+ * order) and d_counts (n_queries x 2: candidates, unique candidates).  These
+ * equal fpp_query_dump's probes and counts (src/FalconnPP.cpp:540-606) in
+ * every precision: only the rerank differs between the forms.  d_out_val,
+ * d_probes and d_counts may be NULL.  No graph is used.  Returns after the
+ * results are written. */
+int fpp_query_batched_dump(fpp_index* h, const float* d_queries, int n_queries, int n_neighbors, int32_t* d_out,
+                           float* d_out_val, uint32_t* d_probes, uint32_t* d_counts, void* stream);
 
 /* Autotuner of the batched form (no reference counterpart).  On a sample of
  * device queries it times the fused kernel over blocks per SM {1,2,3},
@@ -240,21 +256,22 @@ int fpp_load_txt(const char* path, int n_points, int n_features, float* out, lon
 int fpp_output_file(const char* path, const int32_t* topk, int n_queries, int k);
 
 /* No counterpart in the reference.  The gather, deduplicate, rerank and top-k
- * stage of fpp_query for callers that cannot allocate device memory: code
- * recording a CUDA graph, a serving thread that must not stall on cudaMalloc /
- * cudaFree (they synchronise the device), or a host process whose device
- * memory belongs to another allocator.  It allocates nothing: its scratch is
- * a 64 MiB __device__ array that every GPU loading the library holds until
- * exit.  d_queries: n_queries x n_features floats; d_probes: n_queries x
- * n_probes global bucket ids (the probes fpp_query_dump reports); d_out:
- * n_queries x n_neighbors int32, the same top-k fpp_query gives for those
- * probes.  All three in device memory.  The first call on a device looks up
- * the scratch address; make it before any stream capture.  Calls whose
+ * stage of fpp_query for callers that cannot allocate device memory: a
+ * serving thread that must not stall on cudaMalloc / cudaFree (they
+ * synchronise the device), or a host process whose device memory belongs to
+ * another allocator.  It allocates nothing: its scratch is a 64 MiB
+ * __device__ array that every GPU loading the library holds until exit.
+ * d_queries: n_queries x n_features floats; d_probes: n_queries x n_probes
+ * global bucket ids (the probes fpp_query_dump reports); d_out: n_queries x
+ * n_neighbors int32, the same top-k fpp_query gives for those probes.  All
+ * three in device memory.  The first call on a device looks up the scratch
+ * address.  The call waits for its kernel before it returns.  Calls whose
  * kernels overlap on one GPU race on the shared scratch.  Rejects
  * n_neighbors > 1024, n_features > 1024, n_points beyond the scratch (about
- * 500M), and queries with more unique candidates than a block's share
- * (65536 when n_points allows; the row is zeroed and an error returned).
- * Returns after the results are written. */
+ * 500M), probe ids outside [0, n_tables * 4 * n_proj^2) (read as empty
+ * buckets, FPP_ERR_INVALID_ARGUMENT), and queries with more unique
+ * candidates than a block's share (65536 when n_points allows; the row is
+ * zeroed and FPP_ERR_UNSUPPORTED returned). */
 int fpp_rerank_probes_noalloc(fpp_index* h, const float* d_queries, int n_queries, const uint32_t* d_probes,
                               int n_probes, int n_neighbors, int32_t* d_out, void* stream);
 
