@@ -39,10 +39,14 @@ sys.path.insert(0, ROOT)
 
 WORKLOADS = {
     "mips-1Mx200-L100": dict(n=1_000_000, d=200, n_centres=256, norm_sigma=0.4, L=100, D=256, minSize=1000,
-                             alpha=0.01, iProbes=3, nq=10_000, k=20, sweep=(10, 20, 40, 80)),
+                             alpha=0.01, iProbes=3, nq=10_000, k=20, qprobes=10,
+                             sweep=(1, 2, 3, 4, 5, 6, 7, 8, 10, 20, 40, 80)),
+    # tiny case for the host-logic tests (runs on the CPU arm in seconds)
+    "mips-20Kx64-L8-tiny": dict(n=20_000, d=64, n_centres=32, norm_sigma=0.4, L=8, D=64, minSize=50, alpha=0.01,
+                                iProbes=3, nq=500, k=10, qprobes=10, sweep=(10,)),
     # small case of the same kernels for profiler captures (index > L2, ~1 GB on the device)
     "mips-300Kx200-L100-small": dict(n=300_000, d=200, n_centres=256, norm_sigma=0.4, L=100, D=256, minSize=1000,
-                                     alpha=0.01, iProbes=3, nq=2_000, k=20, sweep=(10,)),
+                                     alpha=0.01, iProbes=3, nq=2_000, k=20, qprobes=10, sweep=(10,)),
 }
 INDEX_SEED = 42
 # (form, precision, shortlist multiple): form 0 plain three-kernel path, 1 batched fused kernel
@@ -132,6 +136,18 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+    return platform.processor() or "unknown"
+
+
 def query_seed(rank: int) -> int:
     """Each replica answers its own batch: rank r draws its queries with seed 1 + 1000 r."""
     return 1 + 1000 * rank
@@ -146,6 +162,12 @@ def reduce_max(x: float, device: str = "cuda") -> float:
     t = torch.tensor([x], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def aggregate_qps(world: int, nq: int, steps: int, max_total_ms: float) -> float:
+    """Whole-job queries/s: every replica answers nq queries per step, and
+    the job takes as long as its slowest rank."""
+    return world * nq * steps / (max_total_ms / 1000.0)
 
 
 def make_data(w, rank):
@@ -253,10 +275,36 @@ def run_ours(args, w, rank, world, local_rank):
             torch.cuda.synchronize()
             total_ms = reduce_max(ev0.elapsed_time(ev1))
             idx.set_option("stage_timing", 0)
-            results[fname] = dict(value=world * nq * args.steps / (total_ms / 1000.0), ms=total_ms / args.steps,
+            results[fname] = dict(value=aggregate_qps(world, nq, args.steps, total_ms), ms=total_ms / args.steps,
                                   step_ms=step_ms, launches=launches, recall=r, rerank_ms=rerank_ms)
             if form == 0:
                 plain_stats = (uniq / args.steps, cand / args.steps, statistics.mean(rerank_ms) / 1000.0)
+    # opt-in variant, not the headline: FP8 with the tensor-core rotation
+    # (FP16 operands, so its probes may differ from the reference's FP32 hash)
+    variant = None
+    if args.form == "all":
+        idx.set_query_form(1, 2, 2)
+        idx.set_option("use_graph", 1)
+        idx.set_option("tc_rotation", 1)
+        for _ in range(args.warmup):
+            idx.query_device(Qd.data_ptr(), nq, k, outd.data_ptr(), sp)
+        torch.cuda.synchronize()
+        vr = recall(truth, outd[:ns].cpu().numpy(), k)
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(tstream):
+            ev0.record()
+            for _ in range(args.steps):
+                idx.query_device(Qd.data_ptr(), nq, k, outd.data_ptr(), sp)
+            ev1.record()
+        torch.cuda.synchronize()
+        vms = reduce_max(ev0.elapsed_time(ev1)) / args.steps
+        idx.set_option("tc_rotation", 0)
+        variant = {"batched-fp8-fp16hash": {"value": round(world * nq / (vms / 1000.0), 1), "ms_per_step": round(vms, 4),
+                                            "recall_at_k": round(vr, 4),
+                                            "note": "opt-in tensor-core rotation with FP16 operands: not the "
+                                                    "reference's FP32 hash, excluded from the headline"}}
+
     # headline: the fastest batched form that reaches the recall target
     cands = [f for f in forms if f != "plain-fp32" and results[f]["recall"] >= RECALL_TARGET] or forms
     head = max(cands, key=lambda f: results[f]["value"])
@@ -347,54 +395,90 @@ def run_ours(args, w, rank, world, local_rank):
                      "unique_candidates_per_step": int(U), "candidates_per_step": int(C)},
         "clocks": clk.summary(),
     }
+    if variant:
+        result["variants_not_headline"] = variant
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         result["cpu_baseline"] = cpu_baseline_from_index(idx, X, Q, w, chosen)
     return result
 
 
+class stdout_to_stderr:
+    """The reference's C++ code prints its reports to stdout (cout); send
+    file descriptor 1 to stderr meanwhile, so stdout keeps one JSON line."""
+
+    def __enter__(self):
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        os.dup2(2, 1)
+        return self
+
+    def __exit__(self, *exc):
+        sys.stdout.flush()
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+
+
 def cpu_baseline_from_index(idx, X, Q, w, qprobes):
-    """The oracle's query path (the reference's algorithm on the host cores)
-    on the same index, over the same batch of queries."""
+    """The reference's own query path (src/FalconnPP.cpp:310-707, compiled from
+    its sources into oracle/_ref) on the GPU-built index, over a sample of the
+    step's queries, with every host thread; the oracle port where that build
+    is absent."""
     from oracle import oracle
-    o = oracle.Index(w["n"], w["d"])
     threads = os.cpu_count() or 1
-    o.set_index_param(w["L"], w["D"], w["minSize"], w["alpha"], w["iProbes"], threads, INDEX_SEED)
     center = idx.dump_center()
     b1, b2 = idx.dump_bits()
     start, ids = idx.dump_tables()
     Xc = X - center[None, :]
-    o.import_index(Xc, center, b1, b2, start, ids)
+    if oracle.ref_lib() is not None:
+        o = oracle.Reference(w["n"], w["d"])
+        o.set_index_param(w["L"], w["D"], w["minSize"], w["alpha"], w["iProbes"], threads, INDEX_SEED)
+        o.import_index(Xc, b1, b2, start, ids)
+        kind = "reference"
+    else:
+        o = oracle.Index(w["n"], w["d"])
+        o.set_index_param(w["L"], w["D"], w["minSize"], w["alpha"], w["iProbes"], threads, INDEX_SEED)
+        o.import_index(Xc, center, b1, b2, start, ids)
+        kind = "port"
     o.set_qprobes(qprobes)
     nsamp = min(Q.shape[0], 4000)
-    t0 = time.perf_counter()
-    o.query(Q[:nsamp], w["k"])
-    dt = time.perf_counter() - t0
-    return {"value": round(nsamp / dt, 1), "unit": "queries/s", "cores": threads, "kind": "port",
+    with stdout_to_stderr():
+        t0 = time.perf_counter()
+        o.query(Q[:nsamp], w["k"])
+        dt = time.perf_counter() - t0
+    return {"value": round(nsamp / dt, 1), "unit": "queries/s", "cores": threads, "kind": kind,
+            "cpu_model": cpu_model(),
             "sample": f"{nsamp} of the step's {Q.shape[0]} queries on the same index, qProbes={qprobes}"}
 
 
 def run_reference(args, w):
-    """The reference's CPU path: the oracle port builds its own index on the
-    host cores and answers a bounded sample of the batch per step."""
+    """The reference's CPU path: its own FalconnPP code (src/FalconnPP.cpp
+    build2Layers_1D / query2Layers_1D, compiled from its sources into
+    oracle/_ref, OpenMP over every host thread) builds its index on the host
+    cores and answers a bounded sample of the batch per step; the oracle port
+    where that build is absent."""
     from oracle import oracle
     X, Q = make_data(w, 0)
     threads = os.cpu_count() or 1
-    o = oracle.Index(w["n"], w["d"])
+    if oracle.ref_lib() is not None:
+        o, kind, form = oracle.Reference(w["n"], w["d"]), "reference", "reference CPU path (its own code, OpenMP)"
+    else:
+        o, kind, form = oracle.Index(w["n"], w["d"]), "port", "reference CPU path (oracle port, OpenMP)"
     o.set_index_param(w["L"], w["D"], w["minSize"], w["alpha"], w["iProbes"], threads, INDEX_SEED)
-    t0 = time.perf_counter()
-    o.build(X)
-    build_s = time.perf_counter() - t0
-    qp = args.qprobes or w["sweep"][0]
-    o.set_qprobes(qp)
+    qp = args.qprobes or w["qprobes"]
     nsamp = min(Q.shape[0], 2000)
-    for _ in range(args.warmup):
-        o.query(Q[:200], w["k"])
     ts = []
-    for s in range(args.steps):
-        sl = Q[(s * nsamp) % Q.shape[0]:][:nsamp]
+    with stdout_to_stderr():
         t0 = time.perf_counter()
-        o.query(sl, w["k"])
-        ts.append(time.perf_counter() - t0)
+        o.build(X)
+        build_s = time.perf_counter() - t0
+        o.set_qprobes(qp)
+        for _ in range(args.warmup):
+            o.query(Q[:200], w["k"])
+        for s in range(args.steps):
+            sl = Q[(s * nsamp) % Q.shape[0]:][:nsamp]
+            t0 = time.perf_counter()
+            o.query(sl, w["k"])
+            ts.append(time.perf_counter() - t0)
     total = sum(ts)
     value = nsamp * args.steps / total
     return {
@@ -411,10 +495,10 @@ def run_reference(args, w):
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic",
-        "config": dict(workload_config(args, w, qp), form="reference CPU path (oracle port, OpenMP)",
-                       parallelism=f"host-threads{threads}"),
+        "config": dict(workload_config(args, w, qp), form=form, parallelism=f"host-threads{threads}"),
         "build_s": round(build_s, 2),
-        "cpu_baseline": {"value": round(value, 1), "unit": "queries/s", "cores": threads, "kind": "port",
+        "cpu_baseline": {"value": round(value, 1), "unit": "queries/s", "cores": threads, "kind": kind,
+                         "cpu_model": cpu_model(),
                          "sample": f"{nsamp} of the batch's {w['nq']} queries per step"},
         "e2e": {"value": round(value, 1), "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -685,9 +769,18 @@ def main():
     w = WORKLOADS[args.workload]
     if args.qprobes:
         w = dict(w, sweep=(args.qprobes,))
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        # not launched by torchrun: start one replica process per GPU the same
+        # way the driver does, and pass their exit status through
+        cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={args.gpus}",
+               "--master-addr=127.0.0.1", f"--master-port={29500 + os.getpid() % 1000}",
+               os.path.abspath(__file__), *sys.argv[1:]]
+        return subprocess.run(cmd).returncode
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if world != args.gpus and args.impl == "ours":
+        log(f"bench: --gpus {args.gpus} but WORLD_SIZE={world}; running {world} replica(s)")
     if args.impl == "reference":
         if rank != 0:
             return 0
