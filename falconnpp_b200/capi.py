@@ -21,7 +21,7 @@ EXPORTED = [
     "fpp_dump_tables", "fpp_build_dump_hash", "fpp_query_dump", "fpp_rerank_probes_noalloc",
     "fpp_set_query_form", "fpp_query_batched", "fpp_query_batched_dump", "fpp_autotune",
     "fpp_server_create", "fpp_server_submit", "fpp_server_wait", "fpp_server_stats", "fpp_server_destroy",
-    "fpp_bruteforce_topk_f64", "fpp_save", "fpp_load", "fpp_load_txt", "fpp_output_file",
+    "fpp_bruteforce_topk_f64", "fpp_bruteforce_topk_lowp", "fpp_save", "fpp_load", "fpp_load_txt", "fpp_output_file",
 ]
 
 _lib = None
@@ -72,6 +72,7 @@ def lib() -> ctypes.CDLL:
             "fpp_server_stats": (i32, [vp, vp, i32]),
             "fpp_server_destroy": (None, [vp]),
             "fpp_bruteforce_topk_f64": (i32, [vp, i64, i32, vp, i32, i32, vp, vp, vp]),
+            "fpp_bruteforce_topk_lowp": (i32, [vp, vp, i32, i32, i32, i32, vp, vp, vp]),
             "fpp_save": (i32, [vp, ctypes.c_char_p]),
             "fpp_load": (i32, [vp, ctypes.c_char_p]),
             "fpp_load_txt": (i32, [ctypes.c_char_p, i32, i32, vp, vp]),
@@ -185,6 +186,12 @@ class Index:
                                   ctypes.c_void_p(stream or 0)))
         return dict(ms=rep[0], blocks_per_sm=int(rep[1]), precision=int(rep[2]), shortlist_mult=int(rep[3]),
                     agreement=rep[4], tried=int(rep[5]))
+
+    def bruteforce_lowp(self, q_ptr: int, nq: int, k: int, precision: int, shortlist_mult: int, out_ptr: int,
+                        val_ptr: int | None = None, stream: int | None = None):
+        _check(lib().fpp_bruteforce_topk_lowp(self.h, ctypes.c_void_p(q_ptr), nq, k, precision, shortlist_mult,
+                                              ctypes.c_void_p(out_ptr), ctypes.c_void_p(val_ptr or 0),
+                                              ctypes.c_void_p(stream or 0)))
 
     def info(self) -> dict:
         v = np.zeros(9, np.int64)

@@ -136,13 +136,13 @@ int ensure_lowp_rows(const Params& P, DeviceIndex& di, int mode, cudaStream_t s,
   cudaError_t e;
   if (mode == kRowsBF16) {
     const int ldo = (P.n_features + 7) & ~7;  // 16-byte rows
-    if ((e = cudaMalloc(&di.Xlp, (size_t)n * ldo * 2)) != cudaSuccess) goto fail;
+    if ((e = fpp::dev_malloc(&di.Xlp, (size_t)n * ldo * 2)) != cudaSuccess) goto fail;
     k_rows_bf16<<<nsm * 8, 256, 0, s>>>(di.Xc, n, di.ld, ldo, static_cast<uint16_t*>(di.Xlp));
     di.ld_lp = ldo;
   } else {
     const int ldo = (P.n_features + 15) & ~15;
-    if ((e = cudaMalloc(&di.Xlp, (size_t)n * ldo)) != cudaSuccess) goto fail;
-    if ((e = cudaMalloc(&di.Xlp_scale, sizeof(float) * n)) != cudaSuccess) goto fail;
+    if ((e = fpp::dev_malloc(&di.Xlp, (size_t)n * ldo)) != cudaSuccess) goto fail;
+    if ((e = fpp::dev_malloc(&di.Xlp_scale, sizeof(float) * n)) != cudaSuccess) goto fail;
     k_rows_fp8<<<nsm * 8, 256, 0, s>>>(di.Xc, n, di.ld, ldo, static_cast<uint8_t*>(di.Xlp), di.Xlp_scale);
     di.ld_lp = ldo;
   }
@@ -239,17 +239,17 @@ int batch_query(const Params& P, DeviceIndex& di, BatchWorkspace& bw, const Batc
   // (re)allocate per-block scratch when the shape grows
   if (!bw.bitset || bw.grid < grid || bw.nwords != nwords || bw.cap < cap || bw.fht < F || bw.mmax < mmax) {
     bw.release();
-    if ((e = cudaMalloc(&bw.bitset, sizeof(uint32_t) * (size_t)grid * nwords)) != cudaSuccess) return fail(e, "alloc");
+    if ((e = fpp::dev_malloc(&bw.bitset, sizeof(uint32_t) * (size_t)grid * nwords)) != cudaSuccess) return fail(e, "alloc");
     if ((e = cudaMemsetAsync(bw.bitset, 0, sizeof(uint32_t) * (size_t)grid * nwords, s)) != cudaSuccess)
       return fail(e, "memset");
-    if ((e = cudaMalloc(&bw.uniq, sizeof(uint32_t) * (size_t)grid * cap)) != cudaSuccess) return fail(e, "alloc");
-    if ((e = cudaMalloc(&bw.score, sizeof(uint32_t) * (size_t)grid * cap)) != cudaSuccess) return fail(e, "alloc");
-    if ((e = cudaMalloc(&bw.gdump, sizeof(float) * (size_t)groups * F)) != cudaSuccess) return fail(e, "alloc");
-    if ((e = cudaMalloc(&bw.gheap_v, sizeof(float) * (size_t)groups * std::max(mmax, 1))) != cudaSuccess)
+    if ((e = fpp::dev_malloc(&bw.uniq, sizeof(uint32_t) * (size_t)grid * cap)) != cudaSuccess) return fail(e, "alloc");
+    if ((e = fpp::dev_malloc(&bw.score, sizeof(uint32_t) * (size_t)grid * cap)) != cudaSuccess) return fail(e, "alloc");
+    if ((e = fpp::dev_malloc(&bw.gdump, sizeof(float) * (size_t)groups * F)) != cudaSuccess) return fail(e, "alloc");
+    if ((e = fpp::dev_malloc(&bw.gheap_v, sizeof(float) * (size_t)groups * std::max(mmax, 1))) != cudaSuccess)
       return fail(e, "alloc");
-    if ((e = cudaMalloc(&bw.gheap_i, sizeof(int) * (size_t)groups * std::max(mmax, 1))) != cudaSuccess)
+    if ((e = fpp::dev_malloc(&bw.gheap_i, sizeof(int) * (size_t)groups * std::max(mmax, 1))) != cudaSuccess)
       return fail(e, "alloc");
-    if ((e = cudaMalloc(&bw.counters, sizeof(unsigned) * 4)) != cudaSuccess) return fail(e, "alloc");
+    if ((e = fpp::dev_malloc(&bw.counters, sizeof(unsigned) * 4)) != cudaSuccess) return fail(e, "alloc");
     bw.grid = grid;
     bw.nwords = nwords;
     bw.cap = cap;
@@ -268,9 +268,9 @@ int batch_query(const Params& P, DeviceIndex& di, BatchWorkspace& bw, const Batc
     cudaFree(bw.order);
     bw.okey = bw.ohist = bw.order = nullptr;
     bw.order_cap = 0;
-    if ((e = cudaMalloc(&bw.okey, sizeof(uint32_t) * (size_t)rq.nq)) != cudaSuccess) return fail(e, "alloc");
-    if ((e = cudaMalloc(&bw.order, sizeof(uint32_t) * (size_t)rq.nq)) != cudaSuccess) return fail(e, "alloc");
-    if ((e = cudaMalloc(&bw.ohist, sizeof(uint32_t) * kOrderMaxBins)) != cudaSuccess) return fail(e, "alloc");
+    if ((e = fpp::dev_malloc(&bw.okey, sizeof(uint32_t) * (size_t)rq.nq)) != cudaSuccess) return fail(e, "alloc");
+    if ((e = fpp::dev_malloc(&bw.order, sizeof(uint32_t) * (size_t)rq.nq)) != cudaSuccess) return fail(e, "alloc");
+    if ((e = fpp::dev_malloc(&bw.ohist, sizeof(uint32_t) * kOrderMaxBins)) != cudaSuccess) return fail(e, "alloc");
     if ((e = cudaMemsetAsync(bw.ohist, 0, sizeof(uint32_t) * kOrderMaxBins, s)) != cudaSuccess)
       return fail(e, "memset");
     bw.order_cap = rq.nq;

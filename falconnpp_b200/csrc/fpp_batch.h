@@ -86,6 +86,18 @@ struct BatchWorkspace {
   void release();
 };
 
+// Scratch of the brute-force low-precision block kernel (fpp_bf_lowp.cu):
+// query rows, per-query scales, the per-(query, split) shortlist heaps.
+struct BfWorkspace {
+  unsigned char* qrows = nullptr;
+  float* qscale = nullptr;
+  unsigned long long* heap = nullptr;
+  int* heap_n = nullptr;
+  unsigned* status = nullptr;
+  size_t cap_q = 0, cap_qs = 0, cap_hv = 0, cap_n = 0;
+  void release();
+};
+
 int ensure_lowp_rows(const Params& P, DeviceIndex& di, int mode, cudaStream_t s, Error& err);
 
 int batch_query(const Params& P, DeviceIndex& di, BatchWorkspace& bw, const BatchRequest& rq, cudaStream_t s,

@@ -206,8 +206,8 @@ extern "C" int fpp_bruteforce_topk_f64(const float* d_X, long long n_points, int
   unsigned long long* pkey = nullptr;
   uint32_t* pid = nullptr;
   const size_t np = (size_t)n_queries * slices * k;
-  cudaError_t e = cudaMalloc(&pkey, sizeof(unsigned long long) * np);
-  if (e == cudaSuccess) e = cudaMalloc(&pid, sizeof(uint32_t) * np);
+  cudaError_t e = fpp::dev_malloc(&pkey, sizeof(unsigned long long) * np);
+  if (e == cudaSuccess) e = fpp::dev_malloc(&pid, sizeof(uint32_t) * np);
   if (e != cudaSuccess) {
     cudaFree(pkey);
     return set_last_error(FPP_ERR_OUT_OF_MEMORY, "bruteforce: cannot allocate the partial lists");

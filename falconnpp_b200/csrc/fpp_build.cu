@@ -563,7 +563,7 @@ int upload_flips(const Params& P, const HostBits& bits, DeviceIndex& di, cudaStr
           if (bit == 0) hflips[(((size_t)layer * L + l) * 3 + r) * WORDS + i / 32] |= 1u << (i % 32);
         }
   }
-  FPP_CUDA(cudaMalloc(&di.flips, sizeof(uint32_t) * hflips.size()));
+  FPP_CUDA(fpp::dev_malloc(&di.flips, sizeof(uint32_t) * hflips.size()));
   FPP_CUDA(cudaMemcpyAsync(di.flips, hflips.data(), sizeof(uint32_t) * hflips.size(), cudaMemcpyHostToDevice, s));
   if (F == 256) {
     // the tensor-core rotation (batched low-precision form) reads round 2's
@@ -579,7 +579,7 @@ int upload_flips(const Params& P, const HostBits& bits, DeviceIndex& di, cudaStr
         if ((src[p0 >> 5] >> (p0 & 31)) & 1u) dst[pp >> 5] |= 1u << (pp & 31);
       }
     }
-    FPP_CUDA(cudaMalloc(&di.tflips, sizeof(uint32_t) * htflips.size()));
+    FPP_CUDA(fpp::dev_malloc(&di.tflips, sizeof(uint32_t) * htflips.size()));
     FPP_CUDA(cudaMemcpyAsync(di.tflips, htflips.data(), sizeof(uint32_t) * htflips.size(), cudaMemcpyHostToDevice,
                              s));
   }
@@ -642,14 +642,14 @@ int build_index(const Params& P, const float* X, bool x_on_device, const HostBit
     auto t0 = std::chrono::steady_clock::now();
     const float* Xd = X;
     if (!x_on_device) {
-      FPP_CUDA(cudaMalloc(&Xstage, sizeof(float) * n * d));
+      FPP_CUDA(fpp::dev_malloc(&Xstage, sizeof(float) * n * d));
       FPP_CUDA(cudaMemcpyAsync(Xstage, X, sizeof(float) * n * d, cudaMemcpyHostToDevice, s));
       Xd = Xstage;
     }
-    FPP_CUDA(cudaMalloc(&di.Xc, sizeof(float) * n * ld));
-    FPP_CUDA(cudaMalloc(&di.center, sizeof(float) * d));
-    FPP_CUDA(cudaMalloc(&part, sizeof(float) * nchunks_c * d));
-    FPP_CUDA(cudaMalloc(&d_bad, sizeof(int)));
+    FPP_CUDA(fpp::dev_malloc(&di.Xc, sizeof(float) * n * ld));
+    FPP_CUDA(fpp::dev_malloc(&di.center, sizeof(float) * d));
+    FPP_CUDA(fpp::dev_malloc(&part, sizeof(float) * nchunks_c * d));
+    FPP_CUDA(fpp::dev_malloc(&d_bad, sizeof(int)));
     FPP_CUDA(cudaMemsetAsync(d_bad, 0, sizeof(int), s));
     dim3 g1((unsigned)nchunks_c, (unsigned)((d + 255) / 256));
     k_center_partial<<<g1, 256, 0, s>>>(Xd, n, d, part);
@@ -684,24 +684,24 @@ int build_index(const Params& P, const float* X, bool x_on_device, const HostBit
     err.msg = "build: too many entries per table chunk";
     goto fail;
   }
-  FPP_CUDA(cudaMalloc(&counts, sizeof(uint32_t) * (size_t)L * NB));
+  FPP_CUDA(fpp::dev_malloc(&counts, sizeof(uint32_t) * (size_t)L * NB));
   FPP_CUDA(cudaMemsetAsync(counts, 0, sizeof(uint32_t) * (size_t)L * NB, s));
-  FPP_CUDA(cudaMalloc(&di.bucket_off, sizeof(uint32_t) * ((size_t)L * NB + 1)));
+  FPP_CUDA(fpp::dev_malloc(&di.bucket_off, sizeof(uint32_t) * ((size_t)L * NB + 1)));
   for (int i = 0; i < 2; ++i) {
-    FPP_CUDA(cudaMalloc(&keys[i], sizeof(uint64_t) * std::max(1LL, max_entries)));
-    FPP_CUDA(cudaMalloc(&vals[i], sizeof(uint32_t) * std::max(1LL, max_entries)));
+    FPP_CUDA(fpp::dev_malloc(&keys[i], sizeof(uint64_t) * std::max(1LL, max_entries)));
+    FPP_CUDA(fpp::dev_malloc(&vals[i], sizeof(uint32_t) * std::max(1LL, max_entries)));
   }
-  FPP_CUDA(cudaMalloc(&hist, sizeof(uint32_t) * 256 * (size_t)std::max(1, ntiles_max)));
-  FPP_CUDA(cudaMalloc(&digit_total, sizeof(uint32_t) * 256));
-  FPP_CUDA(cudaMalloc(&segstart, sizeof(uint32_t) * nb_chunk_max));
-  FPP_CUDA(cudaMalloc(&flags, sizeof(uint32_t) * nb_chunk_max));
-  FPP_CUDA(cudaMalloc(&repair, sizeof(uint32_t) * nb_chunk_max));
-  FPP_CUDA(cudaMalloc(&n_repair, sizeof(unsigned int)));
-  FPP_CUDA(cudaMalloc(&blk_cnt, sizeof(unsigned long long) * nblk_max));
-  FPP_CUDA(cudaMalloc(&blk_kept, sizeof(unsigned long long) * nblk_max));
-  FPP_CUDA(cudaMalloc(&d_base, sizeof(unsigned long long)));
-  FPP_CUDA(cudaMalloc(&d_maxkept, sizeof(unsigned int)));
-  FPP_CUDA(cudaMalloc(&d_limited, sizeof(unsigned long long)));
+  FPP_CUDA(fpp::dev_malloc(&hist, sizeof(uint32_t) * 256 * (size_t)std::max(1, ntiles_max)));
+  FPP_CUDA(fpp::dev_malloc(&digit_total, sizeof(uint32_t) * 256));
+  FPP_CUDA(fpp::dev_malloc(&segstart, sizeof(uint32_t) * nb_chunk_max));
+  FPP_CUDA(fpp::dev_malloc(&flags, sizeof(uint32_t) * nb_chunk_max));
+  FPP_CUDA(fpp::dev_malloc(&repair, sizeof(uint32_t) * nb_chunk_max));
+  FPP_CUDA(fpp::dev_malloc(&n_repair, sizeof(unsigned int)));
+  FPP_CUDA(fpp::dev_malloc(&blk_cnt, sizeof(unsigned long long) * nblk_max));
+  FPP_CUDA(fpp::dev_malloc(&blk_kept, sizeof(unsigned long long) * nblk_max));
+  FPP_CUDA(fpp::dev_malloc(&d_base, sizeof(unsigned long long)));
+  FPP_CUDA(fpp::dev_malloc(&d_maxkept, sizeof(unsigned int)));
+  FPP_CUDA(fpp::dev_malloc(&d_limited, sizeof(unsigned long long)));
   FPP_CUDA(cudaMemsetAsync(d_base, 0, sizeof(unsigned long long), s));
   FPP_CUDA(cudaMemsetAsync(d_maxkept, 0, sizeof(unsigned int), s));
   FPP_CUDA(cudaMemsetAsync(d_limited, 0, sizeof(unsigned long long), s));
@@ -764,7 +764,7 @@ int build_index(const Params& P, const float* X, bool x_on_device, const HostBit
       uint64_t cap = std::max<uint64_t>(h_base, ids_capacity * 3 / 2);
       cap = std::min<uint64_t>(std::max<uint64_t>(cap, h_base), std::max<uint64_t>(h_base, (uint64_t)L * n * IP));
       int32_t* nids = nullptr;
-      FPP_CUDA(cudaMalloc(&nids, sizeof(int32_t) * cap));
+      FPP_CUDA(fpp::dev_malloc(&nids, sizeof(int32_t) * cap));
       if (ids_cap && di.n_ids)
         FPP_CUDA(cudaMemcpyAsync(nids, ids_cap, sizeof(int32_t) * di.n_ids, cudaMemcpyDeviceToDevice, s));
       FPP_CUDA(cudaStreamSynchronize(s));
@@ -850,7 +850,7 @@ int build_index(const Params& P, const float* X, bool x_on_device, const HostBit
     st.n_limited = (long long)lim;
     st.points_per_table = (double)h_base / (double)n / (double)L;
   }
-  if (ids_cap == nullptr) FPP_CUDA(cudaMalloc(&ids_cap, sizeof(int32_t)));
+  if (ids_cap == nullptr) FPP_CUDA(fpp::dev_malloc(&ids_cap, sizeof(int32_t)));
   di.ids = ids_cap;
   ids_cap = nullptr;
 

@@ -10,6 +10,7 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <atomic>
 #include <chrono>
 #include <fstream>
 #include <iostream>
@@ -94,14 +95,15 @@ int do_build(fpp_index* h, const float* X, bool on_device, cudaStream_t s, int32
   float* dscores = nullptr;
   const size_t ncodes = (size_t)P.n_tables * P.n_points * P.iProbes;
   if (codes_host) {
-    if (cudaMalloc(&dcodes, sizeof(int32_t) * ncodes) != cudaSuccess ||
-        cudaMalloc(&dscores, sizeof(float) * ncodes) != cudaSuccess) {
+    if (fpp::dev_malloc(&dcodes, sizeof(int32_t) * ncodes) != cudaSuccess ||
+        fpp::dev_malloc(&dscores, sizeof(float) * ncodes) != cudaSuccess) {
       cudaFree(dcodes);
       return fail(FPP_ERR_OUT_OF_MEMORY, "build: cannot allocate the hash-code dump");
     }
   }
   h->ws.release();
   h->bw.release();
+    h->bfw.release();
   h->built = false;
   fpp::Error err{0, ""};
   h->bst = fpp::BuildStats();
@@ -181,6 +183,21 @@ namespace fpp {
 // fpp_last_error().
 int set_last_error(int code, const std::string& msg) { return fail(code, msg); }
 int clear_last_error() { return ok(); }
+
+static std::atomic<long long> g_alloc_countdown{0};
+
+cudaError_t dev_malloc_bytes(void** p, size_t bytes) {
+  long long c = g_alloc_countdown.load();
+  while (c > 0 && !g_alloc_countdown.compare_exchange_weak(c, c - 1)) {
+  }
+  if (c == 1) {  // this is the armed allocation: fail it on the host
+    *p = nullptr;
+    return cudaErrorMemoryAllocation;
+  }
+  return cudaMalloc(p, bytes);
+}
+
+void arm_alloc_failure(long long nth) { g_alloc_countdown.store(nth > 0 ? nth : 0); }
 }  // namespace fpp
 
 extern "C" {
@@ -215,6 +232,7 @@ void fpp_destroy(fpp_index* h) {
     cudaSetDevice(h->device);
     h->ws.release();
     h->bw.release();
+    h->bfw.release();
     fpp::free_index(h->di);
     if (h->stream) cudaStreamDestroy(h->stream);
   }
@@ -271,6 +289,7 @@ int fpp_clear(fpp_index* h) {
   cudaSetDevice(h->device);
   h->ws.release();
   h->bw.release();
+    h->bfw.release();
   fpp::free_index(h->di);
   h->bits = fpp::HostBits();
   h->built = false;
@@ -293,6 +312,9 @@ int fpp_set_option(fpp_index* h, const char* key, long long value) {
     h->blocks_per_sm = (int)value;
   } else if (!strcmp(key, "stage_timing")) {
     h->ws.stage_timing = value != 0;
+  } else if (!strcmp(key, "inject_alloc_failure")) {
+    if (value < 0) return fail(FPP_ERR_INVALID_ARGUMENT, "set_option: inject_alloc_failure must be >= 0");
+    fpp::arm_alloc_failure(value);
   } else if (!strcmp(key, "tables_per_chunk")) {
     if (value < 0) return fail(FPP_ERR_INVALID_ARGUMENT, "set_option: tables_per_chunk must be >= 0");
     h->opt.tables_per_chunk = (int)value;
@@ -345,14 +367,14 @@ int fpp_query(fpp_index* h, const float* queries, int n_queries, int n_neighbors
       cudaFree(h->ws.Qd);
       h->ws.Qd = nullptr;
       h->ws.cap_Qd = 0;
-      e = cudaMalloc(&h->ws.Qd, sizeof(float) * n_queries * P.n_features);
+      e = fpp::dev_malloc(&h->ws.Qd, sizeof(float) * n_queries * P.n_features);
       if (e == cudaSuccess) h->ws.cap_Qd = (size_t)n_queries * P.n_features;
     }
     if (e == cudaSuccess && (size_t)n_queries * n_neighbors > capo) {
       cudaFree(h->ws.out);
       h->ws.out = nullptr;
       h->ws.cap_out = 0;
-      e = cudaMalloc(&h->ws.out, sizeof(int32_t) * n_queries * n_neighbors);
+      e = fpp::dev_malloc(&h->ws.out, sizeof(int32_t) * n_queries * n_neighbors);
       if (e == cudaSuccess) h->ws.cap_out = (size_t)n_queries * n_neighbors;
     }
     if (e != cudaSuccess) return fail(FPP_ERR_OUT_OF_MEMORY, std::string("query: ") + cudaGetErrorString(e));
@@ -442,8 +464,8 @@ int fpp_autotune(fpp_index* h, const float* d_queries, int n_queries, int k, dou
   int32_t* d_ref = nullptr;
   int32_t* d_out = nullptr;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
-  if (cudaMalloc(&d_ref, sizeof(int32_t) * nout) != cudaSuccess ||
-      cudaMalloc(&d_out, sizeof(int32_t) * nout) != cudaSuccess) {
+  if (fpp::dev_malloc(&d_ref, sizeof(int32_t) * nout) != cudaSuccess ||
+      fpp::dev_malloc(&d_out, sizeof(int32_t) * nout) != cudaSuccess) {
     cudaFree(d_ref);
     return fail(FPP_ERR_OUT_OF_MEMORY, "autotune: cannot allocate result buffers");
   }

@@ -18,6 +18,7 @@ struct fpp_index {
   fpp::BuildStats bst;
   fpp::QueryStats qst;
   fpp::BatchWorkspace bw;
+  fpp::BfWorkspace bfw;
   int form = 0;             // 0 plain three-kernel path, 1 batched fused kernel
   int precision = 0;        // batched form: 0 FP32 (exact), 1 BF16, 2 FP8-E4M3
   int shortlist_mult = 4;   // batched low precision: FP32 re-score of shortlist_mult * k

@@ -26,6 +26,17 @@ struct Error {
   std::string msg;
 };
 
+// Every device allocation of the library goes through dev_malloc.  For
+// fault-injection tests on the host, arm_alloc_failure(n) (n >= 1) makes the
+// n-th allocation from then on fail with cudaErrorMemoryAllocation, once,
+// without calling cudaMalloc; n = 0 disarms it.  Process-wide.
+cudaError_t dev_malloc_bytes(void** p, size_t bytes);
+template <typename T>
+inline cudaError_t dev_malloc(T** p, size_t bytes) {
+  return dev_malloc_bytes(reinterpret_cast<void**>(p), bytes);
+}
+void arm_alloc_failure(long long nth);
+
 // Parameters mirror FalconnPP's members (src/FalconnPP.h:14-39).
 struct Params {
   int n_points = 0;

@@ -169,6 +169,7 @@ int fpp_load(fpp_index* h, const char* path) {
   // the handle's old index goes first; on any failure below it stays unbuilt
   h->ws.release();
   h->bw.release();
+    h->bfw.release();
   fpp::free_index(h->di);
   h->built = false;
   fpp::DeviceIndex di;
@@ -177,10 +178,10 @@ int fpp_load(fpp_index* h, const char* path) {
   std::vector<unsigned char> buf(kChunk);
   const uint64_t n = (uint64_t)hd.n_points;
   uint32_t prev = 0, max_kept = 0;
-  bool okr = cudaMalloc(&di.center, sizeof(float) * (size_t)hd.n_features) == cudaSuccess &&
-             cudaMalloc(&di.Xc, sizeof(float) * (size_t)n * hd.ld) == cudaSuccess &&
-             cudaMalloc(&di.bucket_off, sizeof(uint32_t) * (size_t)(hd.n_buckets + 1)) == cudaSuccess &&
-             cudaMalloc(&di.ids, sizeof(int32_t) * std::max<size_t>(1, (size_t)hd.n_ids)) == cudaSuccess;
+  bool okr = fpp::dev_malloc(&di.center, sizeof(float) * (size_t)hd.n_features) == cudaSuccess &&
+             fpp::dev_malloc(&di.Xc, sizeof(float) * (size_t)n * hd.ld) == cudaSuccess &&
+             fpp::dev_malloc(&di.bucket_off, sizeof(uint32_t) * (size_t)(hd.n_buckets + 1)) == cudaSuccess &&
+             fpp::dev_malloc(&di.ids, sizeof(int32_t) * std::max<size_t>(1, (size_t)hd.n_ids)) == cudaSuccess;
   std::string why = okr ? "" : "cannot allocate the index on the device";
   auto any = [](const void*, size_t, size_t) { return true; };
   if (okr) okr = read_device(f, di.center, (size_t)hd.n_features, buf, any) &&

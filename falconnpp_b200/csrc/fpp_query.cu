@@ -573,7 +573,7 @@ static cudaError_t ensure(T*& p, size_t& cap_elems, size_t need) {
   p = nullptr;
   cap_elems = 0;
   const size_t n = std::max<size_t>(need, 1);
-  cudaError_t e = cudaMalloc(&p, n * sizeof(T));
+  cudaError_t e = fpp::dev_malloc(&p, n * sizeof(T));
   if (e == cudaSuccess) cap_elems = n;
   return e;
 }
@@ -724,7 +724,7 @@ int query_index(const Params& P, const DeviceIndex& di, const float* Q, bool q_o
   if (ws.bitset == nullptr || ws.bitset_grid < grid || ws.bitset_words != nwords) {
     cudaFree(ws.bitset);
     ws.bitset = nullptr;
-    if ((e = cudaMalloc(&ws.bitset, sizeof(uint32_t) * (size_t)grid * nwords)) != cudaSuccess)
+    if ((e = fpp::dev_malloc(&ws.bitset, sizeof(uint32_t) * (size_t)grid * nwords)) != cudaSuccess)
       return fail(e, "alloc bitset");
     if ((e = cudaMemsetAsync(ws.bitset, 0, sizeof(uint32_t) * (size_t)grid * nwords, s)) != cudaSuccess)
       return fail(e, "memset bitset");
@@ -757,7 +757,7 @@ int query_index(const Params& P, const DeviceIndex& di, const float* Q, bool q_o
   ra.n_unique = ws.n_unique;
   int32_t* cand_dev = nullptr;
   if (dumps && dumps->want_cands) {
-    if ((e = cudaMalloc(&cand_dev, sizeof(int32_t) * (size_t)nq * cap)) != cudaSuccess)
+    if ((e = fpp::dev_malloc(&cand_dev, sizeof(int32_t) * (size_t)nq * cap)) != cudaSuccess)
       return fail(e, "alloc candidate dump");
     dumps->cand_stride = cap;
   }

@@ -246,10 +246,10 @@ int fpp_server_create(fpp_index* h, int n_streams, long long memory_budget_bytes
   for (Slot& s : S->slots) {
     ok = ok && cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking) == cudaSuccess;
     ok = ok && cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming) == cudaSuccess;
-    ok = ok && cudaMalloc(&s.dQ, sizeof(float) * (size_t)max_batch * d) == cudaSuccess;
-    ok = ok && cudaMalloc(&s.dK, sizeof(int32_t) * max_batch) == cudaSuccess;
-    ok = ok && cudaMalloc(&s.dP, sizeof(int32_t) * max_batch) == cudaSuccess;
-    ok = ok && cudaMalloc(&s.dOut, sizeof(int32_t) * (size_t)max_batch * k_max) == cudaSuccess;
+    ok = ok && fpp::dev_malloc(&s.dQ, sizeof(float) * (size_t)max_batch * d) == cudaSuccess;
+    ok = ok && fpp::dev_malloc(&s.dK, sizeof(int32_t) * max_batch) == cudaSuccess;
+    ok = ok && fpp::dev_malloc(&s.dP, sizeof(int32_t) * max_batch) == cudaSuccess;
+    ok = ok && fpp::dev_malloc(&s.dOut, sizeof(int32_t) * (size_t)max_batch * k_max) == cudaSuccess;
     ok = ok && cudaMallocHost(&s.hQ, sizeof(float) * (size_t)max_batch * d) == cudaSuccess;
     ok = ok && cudaMallocHost(&s.hK, sizeof(int32_t) * max_batch) == cudaSuccess;
     ok = ok && cudaMallocHost(&s.hP, sizeof(int32_t) * max_batch) == cudaSuccess;

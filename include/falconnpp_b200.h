@@ -113,7 +113,10 @@ int fpp_get_stats(fpp_index* h, int kind, double* out, int n);
  * accumulation instead of the reference's FP32 arithmetic; its probes can then
  * differ from the reference's where two rotated coordinates or two bucket
  * scores are within about 1e-3 of each other.  With the default, every form
- * hashes in exact FP32 and probes the reference's buckets). */
+ * hashes in exact FP32 and probes the reference's buckets),
+ * "inject_alloc_failure" (test switch, process-wide: n >= 1 makes the n-th
+ * device allocation from now on fail once with FPP_ERR_OUT_OF_MEMORY, on the
+ * host and without touching the GPU; 0 disarms). */
 int fpp_set_option(fpp_index* h, const char* key, long long value);
 
 /* Prints the build report the reference writes to stdout after
@@ -228,6 +231,20 @@ void fpp_server_destroy(fpp_server* s);
  * written. */
 int fpp_bruteforce_topk_f64(const float* d_X, long long n_points, int n_features, const float* d_Q, int n_queries,
                             int k, int32_t* d_out, double* d_out_val, void* stream);
+
+/* Brute-force block rerank in low precision on the tensor cores (no
+ * reference counterpart; the exact model is BF::mips_topK, src/BF.cpp:17-86).
+ * Scores every indexed point against every query with tcgen05 MMAs over the
+ * index's centred rows in BF16 (precision 1) or FP8-E4M3 with per-row and
+ * per-query FP32 scales (precision 2), FP32 accumulation, keeps the best
+ * k * shortlist_mult per query, re-scores them in exact FP32 (the query
+ * path's dot order) and returns the top k by (score desc, id asc): d_out
+ * n_queries x k int32, d_out_val (may be NULL) the FP32 scores.  d_queries:
+ * n_queries x n_features device floats.  Limits: k * shortlist_mult <= 256,
+ * n_features <= 256 (BF16) / 512 (FP8).  Returns after the results are
+ * written. */
+int fpp_bruteforce_topk_lowp(fpp_index* h, const float* d_queries, int n_queries, int n_neighbors, int precision,
+                             int shortlist_mult, int32_t* d_out, float* d_out_val, void* stream);
 
 /* Index persistence (no counterpart in the reference, which rebuilds its
  * index on every run): fpp_save writes a built index (parameters, sign bits,
