@@ -124,6 +124,10 @@ class Index:
     def set_qprobes(self, q: int):
         _check(lib().fpp_set_qprobes(self.h, q))
 
+    def clear(self):
+        """The reference's clear() (src/FalconnPP.h:102-111): drops the index, keeps the parameters."""
+        _check(lib().fpp_clear(self.h))
+
     def set_option(self, key: str, value: int):
         _check(lib().fpp_set_option(self.h, key.encode(), int(value)))
 

@@ -173,6 +173,15 @@ void BatchWorkspace::release() {
   cudaFree(okey);
   cudaFree(ohist);
   cudaFree(order);
+  cudaFree(glv);
+  cudaFree(glb);
+  cudaFree(gprobe);
+  cudaFree(gpo);
+  cudaFree(gpe);
+  cudaFree(ggv);
+  cudaFree(ggc);
+  cudaFree(grhv);
+  cudaFree(grhi);
   *this = BatchWorkspace();
 }
 
@@ -196,10 +205,13 @@ int batch_query(const Params& P, DeviceIndex& di, BatchWorkspace& bw, const Batc
   const int mmax = (2 * rq.qprobes_max + L - 1) / L;
   int m1max = 0;
   while (m1max * m1max < mmax) ++m1max;
-  if (rq.qprobes_max > kBMaxProbes || (long long)L * mmax > kBMaxList || m1max > kBMaxM1 || m1max > D || L > 512) {
+  // lists, probes and prefixes beyond the shared-memory capacities: the
+  // big-list instances keep them in per-block global scratch
+  const bool big = rq.qprobes_max > kBMaxProbes || (long long)L * mmax > kBMaxList || m1max > kBMaxM1;
+  if (m1max > kBigM1 || m1max > D || L > kBigMaxL || (long long)L * mmax > (1LL << 24)) {
     err.code = kErrUnsupported;
-    err.msg = "batch query: outside the batched form's limits (qProbes <= 1024, n_tables * probes per table <= "
-              "1024, ceil(sqrt(probes per table)) <= 16, n_tables <= 512); use the plain form";
+    err.msg = "batch query: outside the batched form's limits (ceil(sqrt(ceil(2 qProbes / n_tables))) <= "
+              "min(32, n_proj), n_tables <= 512); use the plain form";
     return err.code;
   }
   if (rq.k_max < 1 || (long long)rq.k_max * (rq.mode == kRowsF32 ? 1 : rq.shortlist_mult) > kBMaxTop) {
@@ -213,8 +225,10 @@ int batch_query(const Params& P, DeviceIndex& di, BatchWorkspace& bw, const Batc
   }
   // every query keeps one probe per table (2 qProbes <= L): the kernel
   // without the exact rotation
-  const bool tc_only = rq.tc_rotation && rq.mode != kRowsF32 && F == 256 && di.tflips && 2 * rq.qprobes_max <= L;
-  const KernelSel ks = pick_kernel(F, rq.mode, d, tc_only);
+  const bool tc_only =
+      !big && rq.tc_rotation && rq.mode != kRowsF32 && F == 256 && di.tflips && 2 * rq.qprobes_max <= L;
+  const KernelSel ks = big ? (d > 512 ? KernelSel{nullptr, 0} : pick_kernel_big(F, rq.mode, d))
+                           : pick_kernel(F, rq.mode, d, tc_only);
   const void* kern = ks.fn;
   if (!kern) {
     err.code = kErrUnsupported;
@@ -236,8 +250,11 @@ int batch_query(const Params& P, DeviceIndex& di, BatchWorkspace& bw, const Batc
   const long long cap = std::max<long long>(
       1, std::min<long long>(P.n_points, (long long)rq.qprobes_max * std::max<uint32_t>(di.max_kept, 1u)));
   const int groups = grid * (kBThreads / (F < 32 ? 1 : F / 32));
+  const long long list_cap = big ? (long long)L * mmax : 0;
+  const long long probe_cap = big ? rq.qprobes_max : 0;
   // (re)allocate per-block scratch when the shape grows
-  if (!bw.bitset || bw.grid < grid || bw.nwords != nwords || bw.cap < cap || bw.fht < F || bw.mmax < mmax) {
+  if (!bw.bitset || bw.grid < grid || bw.nwords != nwords || bw.cap < cap || bw.fht < F || bw.mmax < mmax ||
+      bw.list_cap < list_cap || bw.probe_cap < probe_cap) {
     bw.release();
     if ((e = fpp::dev_malloc(&bw.bitset, sizeof(uint32_t) * (size_t)grid * nwords)) != cudaSuccess) return fail(e, "alloc");
     if ((e = cudaMemsetAsync(bw.bitset, 0, sizeof(uint32_t) * (size_t)grid * nwords, s)) != cudaSuccess)
@@ -250,6 +267,22 @@ int batch_query(const Params& P, DeviceIndex& di, BatchWorkspace& bw, const Batc
     if ((e = fpp::dev_malloc(&bw.gheap_i, sizeof(int) * (size_t)groups * std::max(mmax, 1))) != cudaSuccess)
       return fail(e, "alloc");
     if ((e = fpp::dev_malloc(&bw.counters, sizeof(unsigned) * 4)) != cudaSuccess) return fail(e, "alloc");
+    if (big) {
+      const size_t gl = (size_t)grid * list_cap, gp = (size_t)grid * probe_cap;
+      const size_t gg = (size_t)groups * 2 * (kBigM1 + 1), gr = (size_t)groups * kBigM1;
+      if ((e = fpp::dev_malloc(&bw.glv, sizeof(float) * gl)) != cudaSuccess ||
+          (e = fpp::dev_malloc(&bw.glb, sizeof(uint32_t) * gl)) != cudaSuccess ||
+          (e = fpp::dev_malloc(&bw.gprobe, sizeof(uint32_t) * gp)) != cudaSuccess ||
+          (e = fpp::dev_malloc(&bw.gpo, sizeof(uint32_t) * gp)) != cudaSuccess ||
+          (e = fpp::dev_malloc(&bw.gpe, sizeof(uint32_t) * gp)) != cudaSuccess ||
+          (e = fpp::dev_malloc(&bw.ggv, sizeof(float) * gg)) != cudaSuccess ||
+          (e = fpp::dev_malloc(&bw.ggc, sizeof(int) * gg)) != cudaSuccess ||
+          (e = fpp::dev_malloc(&bw.grhv, sizeof(float) * gr)) != cudaSuccess ||
+          (e = fpp::dev_malloc(&bw.grhi, sizeof(int) * gr)) != cudaSuccess)
+        return fail(e, "alloc");
+    }
+    bw.list_cap = list_cap;
+    bw.probe_cap = probe_cap;
     bw.grid = grid;
     bw.nwords = nwords;
     bw.cap = cap;
@@ -337,7 +370,18 @@ int batch_query(const Params& P, DeviceIndex& di, BatchWorkspace& bw, const Batc
   a.work = bw.counters;
   a.status = bw.counters + 1;
   a.order = reorder ? bw.order : nullptr;
-  a.tflips = (rq.tc_rotation && rq.mode != kRowsF32 && F == 256) ? di.tflips : nullptr;
+  a.tflips = (!big && rq.tc_rotation && rq.mode != kRowsF32 && F == 256) ? di.tflips : nullptr;
+  a.glv = bw.glv;
+  a.glb = bw.glb;
+  a.list_cap = bw.list_cap;
+  a.gprobe = bw.gprobe;
+  a.gpo = bw.gpo;
+  a.gpe = bw.gpe;
+  a.probe_cap = bw.probe_cap;
+  a.ggv = bw.ggv;
+  a.ggc = bw.ggc;
+  a.grhv = bw.grhv;
+  a.grhi = bw.grhi;
   a.dump_probes = rq.dump_probes;
   a.dump_counts = rq.dump_counts;
   void* args[] = {&a};

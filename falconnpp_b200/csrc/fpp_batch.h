@@ -79,6 +79,18 @@ struct BatchWorkspace {
   uint32_t* ohist = nullptr;
   uint32_t* order = nullptr;
   long long order_cap = 0;
+  // big-list form scratch (see BatchArgs)
+  float* glv = nullptr;
+  uint32_t* glb = nullptr;
+  long long list_cap = 0;
+  uint32_t* gprobe = nullptr;
+  uint32_t* gpo = nullptr;
+  uint32_t* gpe = nullptr;
+  long long probe_cap = 0;
+  float* ggv = nullptr;
+  int* ggc = nullptr;
+  float* grhv = nullptr;
+  int* grhi = nullptr;
   cudaGraphExec_t graph_exec = nullptr;
   cudaGraph_t graph = nullptr;
   cudaGraphNode_t graph_knode = nullptr;

@@ -21,6 +21,8 @@ constexpr int kBWarps = kBThreads / 32;
 constexpr int kBMaxList = 1024;   // L * m entries held in shared memory
 constexpr int kBMaxProbes = 1024;
 constexpr int kBMaxM1 = 16;
+constexpr int kBigM1 = 32;        // per-layer probes of the big-list form
+constexpr int kBigMaxL = 512;     // tables of the big-list form (its replay heap lives in the top region)
 constexpr int kBMaxTop = 1024;    // k * shortlist multiple, and the replay heaps
 constexpr int kHT = 8192;         // shared-memory hash set for the dedupe (2^13 slots)
 constexpr int kGPerLane = 8;      // candidate ids per lane per gather step
@@ -67,6 +69,20 @@ struct BatchArgs {
   const uint32_t* tflips;  // non-null: rotate on the tensor cores when a query keeps one probe per table
   uint32_t* dump_probes;   // parity dump (nullable): [nq][qprobes_max] probed global bucket ids
   uint32_t* dump_counts;   // parity dump (nullable): [nq][2] candidates, unique candidates
+  // big-list form (qProbes > 1024, L * m > 1024 or m1 > 16): per-block lists,
+  // probes and gather prefixes, per-group layer lists and replay heaps, in
+  // global scratch instead of shared memory
+  float* glv;
+  uint32_t* glb;
+  long long list_cap;
+  uint32_t* gprobe;
+  uint32_t* gpo;
+  uint32_t* gpe;
+  long long probe_cap;
+  float* ggv;
+  int* ggc;
+  float* grhv;
+  int* grhi;
 };
 
 __device__ __forceinline__ int ceil_sqrt_int(int m) {
@@ -256,18 +272,20 @@ __device__ __forceinline__ uint32_t ht_step(uint32_t id) { return ((id * 0x85EBC
 // probe per table), which leaves the exact rotation's registers out.
 enum HashKind : int { kHashAuto = 0, kHashTC = 1 };
 
-template <int FHT, int MODE, int VI, int VI32, int HASH = kHashAuto>
+template <int FHT, int MODE, int VI, int VI32, int HASH = kHashAuto, bool BIGL = false>
 __global__ void __launch_bounds__(kBThreads, MODE == kRowsF32 ? 2 : 3) k_batch_query(BatchArgs a) {
   static_assert(HASH == kHashAuto || (FHT == 256 && MODE != kRowsF32), "tensor-core rotation: fhtDim 256, BF16/FP8");
+  static_assert(!(BIGL && HASH == kHashTC), "the big-list form hashes in FP32");
+  constexpr int M1C = BIGL ? kBigM1 : kBMaxM1;  // per-layer list capacity
   constexpr int E = Geo<FHT>::E;
   constexpr int G = Geo<FHT>::G;
   constexpr int WORDS = Geo<FHT>::WORDS;
   constexpr int GROUPS = kBThreads / G;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   BatchSmem<GROUPS> sm(smem_raw);
-  float* s_lv = sm.lv;
-  uint32_t* s_lb = sm.lb;
-  uint32_t* s_probe = sm.probe;
+  float* s_lv = BIGL ? a.glv + (size_t)blockIdx.x * a.list_cap : sm.lv;
+  uint32_t* s_lb = BIGL ? a.glb + (size_t)blockIdx.x * a.list_cap : sm.lb;
+  uint32_t* s_probe = BIGL ? a.gprobe + (size_t)blockIdx.x * a.probe_cap : sm.probe;
   unsigned long long* s_top = sm.top;
   __shared__ uint32_t hist[256];
   __shared__ uint32_t s_pre, s_rem;
@@ -281,6 +299,11 @@ __global__ void __launch_bounds__(kBThreads, MODE == kRowsF32 ? 2 : 3) k_batch_q
   const int grp = tid / G;
   const unsigned gmask = (G == 32) ? kFullMask : (((1u << G) - 1u) << (lane & ~(G - 1)));
   const long long gid = (long long)blockIdx.x * GROUPS + grp;
+  // the group's two per-layer lists and its replay heap
+  float* grp_v = BIGL ? a.ggv + gid * 2 * (M1C + 1) : sm.gv + grp * 2 * (M1C + 1);
+  int* grp_c = BIGL ? a.ggc + gid * 2 * (M1C + 1) : sm.gc + grp * 2 * (M1C + 1);
+  float* grp_rhv = BIGL ? a.grhv + gid * M1C : sm.rhv + grp * M1C;
+  int* grp_rhi = BIGL ? a.grhi + gid * M1C : sm.rhi + grp * M1C;
   uint32_t* bits = a.bitset + (size_t)blockIdx.x * a.nwords;
   uint32_t* uq = a.uniq + (size_t)blockIdx.x * a.cap;
   uint32_t* sc = a.score + (size_t)blockIdx.x * a.cap;
@@ -382,22 +405,22 @@ __global__ void __launch_bounds__(kBThreads, MODE == kRowsF32 ? 2 : 3) k_batch_q
 #pragma unroll
           for (int e = 0; e < E; ++e) y[e] = xs[e];
           hd3_rotate<FHT>(y, a.flips + ((size_t)(layer * L + lt) * 3) * WORDS, gl);
-          float* lv = sm.gv + (grp * 2 + layer) * (kBMaxM1 + 1);
-          int* lc = sm.gc + (grp * 2 + layer) * (kBMaxM1 + 1);
+          float* lv = grp_v + layer * (M1C + 1);
+          int* lc = grp_c + layer * (M1C + 1);
           const bool ok = group_top_cp_checked<FHT>(y, gl, a.D, a.log2D, m1, cnt, lv, lc);
           if (!ok) {
 #pragma unroll
             for (int e = 0; e < E; ++e) ydump[gl * E + e] = y[e];
             __syncwarp(gmask);
-            if (gl == 0) replay_layer_topp(ydump, a.D, a.log2D, m1, sm.rhv + grp * kBMaxM1, sm.rhi + grp * kBMaxM1, lv, lc);
+            if (gl == 0) replay_layer_topp(ydump, a.D, a.log2D, m1, grp_rhv, grp_rhi, lv, lc);
             __syncwarp(gmask);
           }
         }
         if (gl == 0 && active) {
-          const float* lv1 = sm.gv + (grp * 2 + 0) * (kBMaxM1 + 1);
-          const int* lc1 = sm.gc + (grp * 2 + 0) * (kBMaxM1 + 1);
-          const float* lv2 = sm.gv + (grp * 2 + 1) * (kBMaxM1 + 1);
-          const int* lc2 = sm.gc + (grp * 2 + 1) * (kBMaxM1 + 1);
+          const float* lv1 = grp_v;
+          const int* lc1 = grp_c;
+          const float* lv2 = grp_v + (M1C + 1);
+          const int* lc2 = grp_c + (M1C + 1);
           const uint32_t tbase = (uint32_t)l * a.NB;
           const int twoD = 2 * a.D;
           if (m == 1) {
@@ -421,8 +444,46 @@ __global__ void __launch_bounds__(kBThreads, MODE == kRowsF32 ? 2 : 3) k_batch_q
     __syncthreads();
 
     // ---- 2. global top-qProbes of the L*m lists (FalconnPP.cpp:540-582):
-    // rank by counting; a tie straddling the cut replays the reference's heap
-    {
+    // rank by counting (big lists: radix selection of the qProbes-th largest
+    // score); a tie straddling the cut replays the reference's heap
+    if constexpr (BIGL) {
+      bool tie = false;
+      uint32_t t = 0;
+      if (Qp < M) {
+        unsigned ge;
+        t = block_select(M, (unsigned)Qp, [&](int i) { return ord_key(s_lv[i]); }, hist, &s_pre, &s_rem, &s_cnt, &ge);
+        tie = ge != (unsigned)Qp;
+      }
+      if (!tie) {
+        long long run = 0;
+        for (int base = 0; base < M; base += kBThreads) {
+          const int i = base + tid;
+          const bool take = i < M && (Qp >= M || ord_key(s_lv[i]) >= t);
+          long long tot;
+          const long long pos = block_exclusive_scan(take ? 1 : 0, tmp, &tot) + run;
+          if (take) s_probe[pos] = s_lb[i];
+          run += tot;
+        }
+      } else if (tid == 0) {
+        float* hv = sm.phv();
+        int* hi = sm.phi();
+        int* track = hi + L;
+        int n = 0;
+        for (int l = 0; l < L; ++l) {
+          heap_push<false, int>(hv, hi, n, s_lv[l * m], l * m);
+          track[l] = 0;
+        }
+        for (int pc = 0; pc < Qp; ++pc) {
+          const int pos = hi[0];
+          heap_pop<false, int>(hv, hi, n);
+          s_probe[pc] = s_lb[pos];
+          const int tb = pos / m;
+          track[tb]++;
+          if (track[tb] < m) heap_push<false, int>(hv, hi, n, s_lv[tb * m + track[tb]], tb * m + track[tb]);
+        }
+      }
+      __syncthreads();
+    } else {
       // the order keys of the scores, once, in the top-k region (free until
       // the replay below, which runs after the counting), padded with key 0
       // to a multiple of 4 (scores are >= 0, so their keys exceed 0)
@@ -477,8 +538,8 @@ __global__ void __launch_bounds__(kBThreads, MODE == kRowsF32 ? 2 : 3) k_batch_q
     // ---- 3. gather + dedupe (FalconnPP.cpp:584-606): the candidates of all
     // probes flattened over the warps; dedupe in a shared-memory hash set, or
     // (when a query has too many unique ids) in the block's L2 bitset
-    uint32_t* s_po = sm.po();
-    uint32_t* s_pe = sm.pe();
+    uint32_t* s_po = BIGL ? a.gpo + (size_t)blockIdx.x * a.probe_cap : sm.po();
+    uint32_t* s_pe = BIGL ? a.gpe + (size_t)blockIdx.x * a.probe_cap : sm.pe();
     {
       long long run = 0;
       for (int base = 0; base < Qp; base += kBThreads) {
@@ -840,22 +901,22 @@ struct KernelSel {
   size_t smem;
 };
 
-template <int FHT, int MODE, int VI, int VI32, int HASH = kHashAuto>
+template <int FHT, int MODE, int VI, int VI32, int HASH = kHashAuto, bool BIGL = false>
 static KernelSel kernel_ptr() {
-  const void* fn = reinterpret_cast<const void*>(&k_batch_query<FHT, MODE, VI, VI32, HASH>);
+  const void* fn = reinterpret_cast<const void*>(&k_batch_query<FHT, MODE, VI, VI32, HASH, BIGL>);
   const size_t smem = batch_smem_bytes<FHT>();
   cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   return KernelSel{fn, smem};
 }
 
-template <int MODE, int VI, int VI32>
+template <int MODE, int VI, int VI32, bool BIGL = false>
 static KernelSel pick_fht(int fht) {
   switch (fht) {
-    case 32: return kernel_ptr<32, MODE, VI, VI32>();
-    case 64: return kernel_ptr<64, MODE, VI, VI32>();
-    case 128: return kernel_ptr<128, MODE, VI, VI32>();
-    case 256: return kernel_ptr<256, MODE, VI, VI32>();
-    case 512: return kernel_ptr<512, MODE, VI, VI32>();
+    case 32: return kernel_ptr<32, MODE, VI, VI32, kHashAuto, BIGL>();
+    case 64: return kernel_ptr<64, MODE, VI, VI32, kHashAuto, BIGL>();
+    case 128: return kernel_ptr<128, MODE, VI, VI32, kHashAuto, BIGL>();
+    case 256: return kernel_ptr<256, MODE, VI, VI32, kHashAuto, BIGL>();
+    case 512: return kernel_ptr<512, MODE, VI, VI32, kHashAuto, BIGL>();
     default: return KernelSel{nullptr, 0};
   }
 }
@@ -865,6 +926,7 @@ static KernelSel pick_fht(int fht) {
 KernelSel pick_kernel_f32(int fht, int d);
 KernelSel pick_kernel_bf16(int fht, int d, bool tc_only);
 KernelSel pick_kernel_fp8(int fht, int d, bool tc_only);
+KernelSel pick_kernel_big(int fht, int mode, int d);  // fpp_batch_big.cu
 
 inline int vi_of(int d, int epc) {
   const int v = ((d + epc - 1) / epc + 31) / 32;

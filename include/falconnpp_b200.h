@@ -167,8 +167,10 @@ int fpp_set_query_form(fpp_index* h, int form, int precision, int shortlist_mult
  * n_queries x out_stride int32 (first k of each row written, descending
  * score, 0-padded), d_out_val the matching scores or NULL.  Uses the handle's
  * precision and shortlist setting.  Returns after the results are written.
- * Limits: qProbes <= 1024, n_tables * ceil(2 qProbes / n_tables) <= 2048,
- * k * shortlist_mult <= 1024. */
+ * Limits: ceil(sqrt(ceil(2 qProbes / n_tables))) <= min(32, n_proj),
+ * n_tables <= 512, k * shortlist_mult <= 1024.  Batches with qProbes > 1024,
+ * n_tables * ceil(2 qProbes / n_tables) > 1024 or more than 16 probes per
+ * layer run the big-list instances, whose lists live in global scratch. */
 int fpp_query_batched(fpp_index* h, const float* d_queries, int n_queries, const int32_t* d_k,
                       const int32_t* d_qprobes, int k_max, int qprobes_max, int32_t* d_out, int out_stride,
                       float* d_out_val, void* stream);
