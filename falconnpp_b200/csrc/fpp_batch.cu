@@ -25,6 +25,7 @@
 #include <vector>
 
 #include "fpp_batch_kernel.cuh"
+#include "fpp_query.h"
 
 namespace fpp {
 
@@ -110,6 +111,16 @@ __global__ void __launch_bounds__(1024) k_order_scatter(const uint32_t* __restri
   for (int q = t; q < nq; q += blockDim.x) order[atomicAdd(&off[key[q]], 1u)] = (uint32_t)q;
 }
 
+// the key from the exact lists: the first-layer code of table 0's best bucket
+__global__ void k_order_key_ext(const uint32_t* __restrict__ lb, int nq, long long stride, int twoD,
+                                uint32_t* __restrict__ key, uint32_t* __restrict__ hist) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= nq) return;
+  const uint32_t c = lb[(size_t)q * stride] / (uint32_t)twoD;  // table 0: global id = c1 * 2D + c2
+  key[q] = c;
+  atomicAdd(hist + c, 1u);
+}
+
 static const void* order_key_kernel(int fht) {
   switch (fht) {
     case 32: return reinterpret_cast<const void*>(&k_order_key<32>);
@@ -182,6 +193,10 @@ void BatchWorkspace::release() {
   cudaFree(ggc);
   cudaFree(grhv);
   cudaFree(grhi);
+  cudaFree(ext_lv);
+  cudaFree(ext_lb);
+  cudaFree(hheap_v);
+  cudaFree(hheap_i);
   *this = BatchWorkspace();
 }
 
@@ -227,8 +242,12 @@ int batch_query(const Params& P, DeviceIndex& di, BatchWorkspace& bw, const Batc
   // without the exact rotation
   const bool tc_only =
       !big && rq.tc_rotation && rq.mode != kRowsF32 && F == 256 && di.tflips && 2 * rq.qprobes_max <= L;
-  const KernelSel ks = big ? (d > 512 ? KernelSel{nullptr, 0} : pick_kernel_big(F, rq.mode, d))
-                           : pick_kernel(F, rq.mode, d, tc_only);
+  // the exact hash in its own kernel (k_query_hash with per-query qProbes),
+  // then the fused kernel without the rotation compiled in
+  const bool split = rq.split_hash && !tc_only && d <= 512;
+  const KernelSel ks = split ? pick_kernel_ext(rq.mode, d, big)
+                       : big ? (d > 512 ? KernelSel{nullptr, 0} : pick_kernel_big(F, rq.mode, d))
+                             : pick_kernel(F, rq.mode, d, tc_only);
   const void* kern = ks.fn;
   if (!kern) {
     err.code = kErrUnsupported;
@@ -290,6 +309,37 @@ int batch_query(const Params& P, DeviceIndex& di, BatchWorkspace& bw, const Batc
     bw.mmax = std::max(mmax, 1);
   }
   grid = std::min(grid, bw.grid);
+  const long long ext_stride = (long long)L * std::max(mmax, 1);
+  if (split) {
+    const long long max_groups = (long long)nsm * 64;
+    if (!bw.ext_lv || bw.ext_cap < (long long)rq.nq * ext_stride) {
+      cudaFree(bw.ext_lv);
+      cudaFree(bw.ext_lb);
+      bw.ext_lv = nullptr;
+      bw.ext_lb = nullptr;
+      bw.ext_cap = 0;
+      const size_t ne = (size_t)rq.nq * ext_stride;
+      if ((e = fpp::dev_malloc(&bw.ext_lv, sizeof(float) * ne)) != cudaSuccess ||
+          (e = fpp::dev_malloc(&bw.ext_lb, sizeof(uint32_t) * ne)) != cudaSuccess)
+        return fail(e, "alloc");
+      bw.ext_cap = (long long)ne;
+    }
+    if (!bw.hheap_v || bw.hheap_cap < max_groups * std::max(mmax, 1)) {
+      cudaFree(bw.hheap_v);
+      cudaFree(bw.hheap_i);
+      bw.hheap_v = nullptr;
+      bw.hheap_i = nullptr;
+      bw.hheap_cap = 0;
+      const size_t nh = (size_t)max_groups * std::max(mmax, 1);
+      if ((e = fpp::dev_malloc(&bw.hheap_v, sizeof(float) * nh)) != cudaSuccess ||
+          (e = fpp::dev_malloc(&bw.hheap_i, sizeof(int) * nh)) != cudaSuccess)
+        return fail(e, "alloc");
+      bw.hheap_cap = (long long)nh;
+    }
+    if ((e = hash_lists(P, di, rq.Q, rq.nq, rq.q_qprobes, rq.qprobes_max, bw.ext_lv, bw.ext_lb, ext_stride,
+                        bw.hheap_v, bw.hheap_i, max_groups, s)) != cudaSuccess)
+      return fail(e, "hash kernel");
+  }
   // query order (worth it once the batch is a few waves of blocks)
   int log2D = 0;
   while ((1 << log2D) < D) ++log2D;
@@ -308,7 +358,12 @@ int batch_query(const Params& P, DeviceIndex& di, BatchWorkspace& bw, const Batc
       return fail(e, "memset");
     bw.order_cap = rq.nq;
   }
-  if (reorder) {
+  if (reorder && split) {
+    k_order_key_ext<<<(rq.nq + 255) / 256, 256, 0, s>>>(bw.ext_lb, rq.nq, ext_stride, 2 * D, bw.okey, bw.ohist);
+    if ((e = cudaGetLastError()) != cudaSuccess) return fail(e, "order key launch");
+    k_order_scatter<<<1, 1024, 0, s>>>(bw.okey, rq.nq, 2 * D, bw.ohist, bw.order);
+    if ((e = cudaGetLastError()) != cudaSuccess) return fail(e, "order scatter launch");
+  } else if (reorder) {
     const int per_block = 256 / (F / 32);
     const float* q_ptr = rq.Q;
     int nq_arg = rq.nq, d_arg = d, D_arg = D, l2_arg = log2D, bins = 2 * D;
@@ -384,6 +439,9 @@ int batch_query(const Params& P, DeviceIndex& di, BatchWorkspace& bw, const Batc
   a.grhi = bw.grhi;
   a.dump_probes = rq.dump_probes;
   a.dump_counts = rq.dump_counts;
+  a.ext_lv = bw.ext_lv;
+  a.ext_lb = bw.ext_lb;
+  a.ext_stride = ext_stride;
   void* args[] = {&a};
 
   const bool can_graph = rq.use_graph && !rq.dump_probes && !rq.dump_counts;
@@ -444,7 +502,7 @@ int batch_query(const Params& P, DeviceIndex& di, BatchWorkspace& bw, const Batc
         return fail(e, "launch");
     }
   }
-  res.launches = reorder ? 3 : 1;
+  res.launches = (reorder ? 3 : 1) + (split ? 1 : 0);
   res.grid = grid;
   if (rq.check_status) {
     unsigned st[2] = {0, 0};

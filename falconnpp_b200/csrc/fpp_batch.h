@@ -25,6 +25,7 @@ struct BatchRequest {
   bool reorder = true;             // process the queries grouped by a locality key
   uint32_t* dump_probes = nullptr;  // parity dumps (device, nullable; no graph): [nq][qprobes_max] probes
   uint32_t* dump_counts = nullptr;  // [nq][2] candidates, unique candidates
+  bool split_hash = true;           // exact hash in its own kernel before the fused one (kHashExt)
   bool tc_rotation = false;        // opt-in, BF16/FP8, fhtDim 256: rotate on the tensor cores (FP16 operands,
                                    // not the reference's FP32 hash: probes can differ)
 };
@@ -91,6 +92,13 @@ struct BatchWorkspace {
   int* ggc = nullptr;
   float* grhv = nullptr;
   int* grhi = nullptr;
+  // split hash: per-query lists and the hash kernel's pair-heap scratch
+  float* ext_lv = nullptr;
+  uint32_t* ext_lb = nullptr;
+  long long ext_cap = 0;
+  float* hheap_v = nullptr;
+  int* hheap_i = nullptr;
+  long long hheap_cap = 0;
   cudaGraphExec_t graph_exec = nullptr;
   cudaGraph_t graph = nullptr;
   cudaGraphNode_t graph_knode = nullptr;

@@ -83,6 +83,10 @@ struct BatchArgs {
   int* ggc;
   float* grhv;
   int* grhi;
+  // kHashExt: the per-table lists of query q at ext_lv / ext_lb + q * ext_stride
+  const float* ext_lv;
+  const uint32_t* ext_lb;
+  long long ext_stride;
 };
 
 __device__ __forceinline__ int ceil_sqrt_int(int m) {
@@ -269,12 +273,16 @@ __device__ __forceinline__ uint32_t ht_step(uint32_t id) { return ((id * 0x85EBC
 // HASH: kHashAuto rotates on the tensor cores where a query keeps one probe
 // per table (and a.tflips is set), exactly otherwise; kHashTC only on the
 // tensor cores (the host uses it when every query of the batch keeps one
-// probe per table), which leaves the exact rotation's registers out.
-enum HashKind : int { kHashAuto = 0, kHashTC = 1 };
+// probe per table), which leaves the exact rotation's registers out;
+// kHashExt takes every query's per-table probe lists from the exact FP32
+// hash kernel launched before it (hash_lists, the plain path's k_query_hash
+// with per-query qProbes), so the rotation's registers and spills leave the
+// gather / rerank loop entirely.
+enum HashKind : int { kHashAuto = 0, kHashTC = 1, kHashExt = 2 };
 
 template <int FHT, int MODE, int VI, int VI32, int HASH = kHashAuto, bool BIGL = false>
 __global__ void __launch_bounds__(kBThreads, MODE == kRowsF32 ? 2 : 3) k_batch_query(BatchArgs a) {
-  static_assert(HASH == kHashAuto || (FHT == 256 && MODE != kRowsF32), "tensor-core rotation: fhtDim 256, BF16/FP8");
+  static_assert(HASH != kHashTC || (FHT == 256 && MODE != kRowsF32), "tensor-core rotation: fhtDim 256, BF16/FP8");
   static_assert(!(BIGL && HASH == kHashTC), "the big-list form hashes in FP32");
   constexpr int M1C = BIGL ? kBigM1 : kBMaxM1;  // per-layer list capacity
   constexpr int E = Geo<FHT>::E;
@@ -334,6 +342,10 @@ __global__ void __launch_bounds__(kBThreads, MODE == kRowsF32 ? 2 : 3) k_batch_q
     const int m1 = ceil_sqrt_int(m);     // ceil(sqrt(m)), FalconnPP.cpp:337
     const int M = L * m;
     const float* qv = a.Q + (size_t)q * a.d;
+    if constexpr (HASH == kHashExt) {
+      s_lv = const_cast<float*>(a.ext_lv) + (size_t)q * a.ext_stride;
+      s_lb = const_cast<uint32_t*>(a.ext_lb) + (size_t)q * a.ext_stride;
+    }
     {
       float amax = 0.0f;  // max |q| (the E4M3 query scale)
       for (int i = tid; i < 1024; i += kBThreads) {
@@ -351,7 +363,7 @@ __global__ void __launch_bounds__(kBThreads, MODE == kRowsF32 ? 2 : 3) k_batch_q
     __syncthreads();
 
     // ---- 1. rotate + hash every table (FalconnPP.cpp:358-531)
-    if (FHT == 256 && MODE != kRowsF32 && (HASH == kHashTC || (a.tflips && m == 1))) {
+    if (HASH != kHashExt && FHT == 256 && MODE != kRowsF32 && (HASH == kHashTC || (a.tflips && m == 1))) {
       // low-precision modes with one probe per table: each warp rotates one
       // (table, layer) at a time on the tensor cores and keeps its best
       // coordinate (ties to the smaller position)
@@ -927,6 +939,7 @@ KernelSel pick_kernel_f32(int fht, int d);
 KernelSel pick_kernel_bf16(int fht, int d, bool tc_only);
 KernelSel pick_kernel_fp8(int fht, int d, bool tc_only);
 KernelSel pick_kernel_big(int fht, int mode, int d);  // fpp_batch_big.cu
+KernelSel pick_kernel_ext(int mode, int d, bool big);  // fpp_batch_ext.cu
 
 inline int vi_of(int d, int epc) {
   const int v = ((d + epc - 1) / epc + 31) / 32;

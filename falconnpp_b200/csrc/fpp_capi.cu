@@ -164,6 +164,7 @@ int run_batched(fpp_index* h, const float* dQ, int nq, int k, int32_t* dout, cud
   rq.blocks_per_sm = h->blocks_per_sm;
   rq.reorder = h->reorder;
   rq.tc_rotation = h->tc_rotation;
+  rq.split_hash = h->split_hash;
   rq.check_status = check_status;
   fpp::BatchResult res;
   fpp::Error err{0, ""};
@@ -307,6 +308,8 @@ int fpp_set_option(fpp_index* h, const char* key, long long value) {
     h->reorder = value != 0;
   } else if (!strcmp(key, "tc_rotation")) {
     h->tc_rotation = value != 0;
+  } else if (!strcmp(key, "split_hash")) {
+    h->split_hash = value != 0;
   } else if (!strcmp(key, "blocks_per_sm")) {
     if (value < 0) return fail(FPP_ERR_INVALID_ARGUMENT, "set_option: blocks_per_sm must be >= 0");
     h->blocks_per_sm = (int)value;
@@ -487,6 +490,7 @@ int fpp_autotune(fpp_index* h, const float* d_queries, int n_queries, int k, dou
     rq.blocks_per_sm = bps;
     rq.reorder = h->reorder;
     rq.tc_rotation = h->tc_rotation;
+  rq.split_hash = h->split_hash;
     rq.check_status = true;
     fpp::BatchResult res;
     fpp::Error err{0, ""};
@@ -598,6 +602,7 @@ int fpp_query_batched(fpp_index* h, const float* d_queries, int n_queries, const
   rq.blocks_per_sm = h->blocks_per_sm;
   rq.reorder = h->reorder;
   rq.tc_rotation = h->tc_rotation;
+  rq.split_hash = h->split_hash;
   rq.check_status = true;
   fpp::BatchResult res;
   fpp::Error err{0, ""};
@@ -636,6 +641,7 @@ int fpp_query_batched_dump(fpp_index* h, const float* d_queries, int n_queries, 
   rq.blocks_per_sm = h->blocks_per_sm;
   rq.reorder = h->reorder;
   rq.tc_rotation = h->tc_rotation;
+  rq.split_hash = h->split_hash;
   rq.dump_probes = d_probes;
   rq.dump_counts = d_counts;
   rq.check_status = true;

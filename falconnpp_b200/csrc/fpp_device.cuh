@@ -32,35 +32,42 @@ struct Geo {
 
 __device__ __forceinline__ uint32_t ord_key(float f) { return ord_key_bits(__float_as_uint(f)); }
 
+// Two butterflies at once with Blackwell's packed FP32 instructions
+// (add.rn.f32x2 / sub.rn.f32x2: each component rounds exactly like a scalar
+// add / sub): (a0, a1) <- (a0 + b0, a1 + b1), (b0, b1) <- (a0 - b0, a1 - b1).
+// Written in inline PTX over scalar registers: with the float2 intrinsics the
+// compiler kept the lane's vector in local memory in some callers.
+__device__ __forceinline__ void f32x2_butterfly(float& a0, float& a1, float& b0, float& b1) {
+  asm("{\n .reg .b64 ra, rb, rs, rd;\n mov.b64 ra, {%0, %1};\n mov.b64 rb, {%2, %3};\n"
+      " add.rn.f32x2 rs, ra, rb;\n sub.rn.f32x2 rd, ra, rb;\n mov.b64 {%0, %1}, rs;\n mov.b64 {%2, %3}, rd;\n}"
+      : "+f"(a0), "+f"(a1), "+f"(b0), "+f"(b1));
+}
+
+// (y0, y1) <- (sg * y0 + o0, sg * y1 + o1) in one packed fma; with sg = +1
+// or -1 the product is exact, so each component rounds like y + o or o - y.
+__device__ __forceinline__ void f32x2_fma_sign(float& y0, float& y1, float sg, float o0, float o1) {
+  asm("{\n .reg .b64 rs, ry, ro, rr;\n mov.b64 rs, {%2, %2};\n mov.b64 ry, {%0, %1};\n mov.b64 ro, {%3, %4};\n"
+      " fma.rn.f32x2 rr, rs, ry, ro;\n mov.b64 {%0, %1}, rr;\n}"
+      : "+f"(y0), "+f"(y1)
+      : "f"(sg), "f"(o0), "f"(o1));
+}
+
 // In-place FWHT of the group's vector, stages in increasing stride.
 //
 // With 32 elements per lane, elements j and j + 16 travel as one pair through
-// Blackwell's packed FP32 instructions (__fadd2_rn / __ffma2_rn: each
-// component rounds exactly like __fadd_rn / __fmaf_rn), so every stage except
-// h = 16 (which pairs j with j + 16 itself) issues half the instructions.
-// The difference a - b is fma(-1, b, a): the product is exact, so its single
-// rounding is that of the subtraction (zeros included).
+// the packed instructions above, so every stage except h = 16 (which pairs j
+// with j + 16 itself) issues half the arithmetic instructions.
 template <int FHT>
 __device__ __forceinline__ void fwht_group(float (&y)[Geo<FHT>::E], int gl) {
   constexpr int E = Geo<FHT>::E;
   constexpr int G = Geo<FHT>::G;
   if constexpr (E == 32) {
-    const float2 neg = make_float2(-1.0f, -1.0f);
 #pragma unroll
     for (int h = 1; h < 16; h <<= 1) {
 #pragma unroll
       for (int i = 0; i < 16; i += 2 * h) {
 #pragma unroll
-        for (int j = i; j < i + h; ++j) {
-          const float2 a = make_float2(y[j], y[j + 16]);
-          const float2 b = make_float2(y[j + h], y[j + h + 16]);
-          const float2 sum = __fadd2_rn(a, b);
-          const float2 dif = __ffma2_rn(neg, b, a);
-          y[j] = sum.x;
-          y[j + 16] = sum.y;
-          y[j + h] = dif.x;
-          y[j + h + 16] = dif.y;
-        }
+        for (int j = i; j < i + h; ++j) f32x2_butterfly(y[j], y[j + 16], y[j + h], y[j + h + 16]);
       }
     }
 #pragma unroll
@@ -73,13 +80,11 @@ __device__ __forceinline__ void fwht_group(float (&y)[Geo<FHT>::E], int gl) {
 #pragma unroll
     for (int s = 1; s < G; s <<= 1) {
       const float sg = (gl & s) ? -1.0f : 1.0f;
-      const float2 sgn2 = make_float2(sg, sg);
 #pragma unroll
       for (int e = 0; e < 16; ++e) {
-        const float2 o = make_float2(__shfl_xor_sync(kFullMask, y[e], s), __shfl_xor_sync(kFullMask, y[e + 16], s));
-        const float2 r = __ffma2_rn(sgn2, make_float2(y[e], y[e + 16]), o);
-        y[e] = r.x;
-        y[e + 16] = r.y;
+        const float o0 = __shfl_xor_sync(kFullMask, y[e], s);
+        const float o1 = __shfl_xor_sync(kFullMask, y[e + 16], s);
+        f32x2_fma_sign(y[e], y[e + 16], sg, o0, o1);
       }
     }
     return;

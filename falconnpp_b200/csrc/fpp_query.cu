@@ -41,6 +41,12 @@ struct QHashArgs {
   int m, m1;
   float* list_v;      // [nq][L][m]
   uint32_t* list_b;   // [nq][L][m] global bucket ids
+  // batched form (nullable): per-query qProbes, clamped to [1, qp_max]; each
+  // query then keeps its own m = ceil(2 qProbes / L) probes per table at
+  // list_v + q * stride + l * m (m above is the largest, stride = L * m)
+  const int* q_qprobes;
+  int qp_max;
+  long long stride;
 };
 
 template <int FHT>
@@ -71,21 +77,32 @@ __global__ void __launch_bounds__(128, 4) k_query_hash(QHashArgs a, float* heap_
   float* hv = reinterpret_cast<float*>(lc2 + (kMaxM1 + 1));
   int* hi = reinterpret_cast<int*>(hv + kMaxM1);
 
-  const int m = a.m, m1 = a.m1;
-  const int cnt = min(m1 + 1, a.D);
+  const int m_all = a.m, m1_all = a.m1;
   const long long items = (long long)a.nq * a.L;
   const long long groups_total = (long long)gridDim.x * GROUPS;
   const long long n_iter = (items + groups_total - 1) / groups_total;
   const long long gid = (long long)blockIdx.x * GROUPS + grp;
   // per-group pair heap (size m) lives in global scratch when m is large
-  float* ph_v = heap_v + gid * (long long)m;
-  int* ph_i = heap_i + gid * (long long)m;
+  float* ph_v = heap_v + gid * (long long)m_all;
+  int* ph_i = heap_i + gid * (long long)m_all;
   for (long long it = 0; it < n_iter; ++it) {
     const long long item = it * groups_total + gid;
     const bool active = item < items;
     const long long itm = active ? item : 0;
     const int q = (int)(itm / a.L);
     const int l = (int)(itm - (long long)q * a.L);
+    int m = m_all, m1 = m1_all;
+    if (a.q_qprobes) {
+      const int qp = min(max(a.q_qprobes[q], 1), a.qp_max);
+      m = (2 * qp + a.L - 1) / a.L;  // ceil(2.0 * qProbes / L)
+      m1 = 0;
+      while (m1 * m1 < m) ++m1;      // ceil(sqrt(m))
+    }
+    // the selection runs warp-uniform (its shuffles span the warp): the
+    // largest m1 of the warp's groups; a group with a smaller m1 then checks
+    // strictness over more entries than it needs, which can only add replays
+    const int m1w = a.q_qprobes ? __reduce_max_sync(kFullMask, m1) : m1;
+    const int cnt = min(m1w + 1, a.D);
     float xr[E];
 #pragma unroll
     for (int e = 0; e < E; ++e) {
@@ -100,7 +117,7 @@ __global__ void __launch_bounds__(128, 4) k_query_hash(QHashArgs a, float* heap_
       hd3_rotate<FHT>(y, a.flips + ((size_t)(layer * a.L + l) * 3) * WORDS, gl);
       float* lv = layer == 0 ? lv1 : lv2;
       int* lc = layer == 0 ? lc1 : lc2;
-      const bool ok = group_top_cp_checked<FHT>(y, gl, a.D, a.log2D, m1, cnt, lv, lc);
+      const bool ok = group_top_cp_checked<FHT>(y, gl, a.D, a.log2D, m1w, cnt, lv, lc);
       if (!ok) {
 #pragma unroll
         for (int e = 0; e < E; ++e) ydump[gl * E + e] = y[e];
@@ -110,8 +127,8 @@ __global__ void __launch_bounds__(128, 4) k_query_hash(QHashArgs a, float* heap_
       }
     }
     if (gl == 0 && active) {
-      float* ov = a.list_v + ((size_t)q * a.L + l) * m;
-      uint32_t* ob = a.list_b + ((size_t)q * a.L + l) * m;
+      float* ov = a.list_v + (size_t)q * a.stride + (size_t)l * m;
+      uint32_t* ob = a.list_b + (size_t)q * a.stride + (size_t)l * m;
       const uint32_t tbase = (uint32_t)l * a.NB;
       const int twoD = 2 * a.D;
       if (m == 1) {
@@ -566,6 +583,36 @@ static cudaError_t dispatch_qhash(int fht, const QHashArgs& a, int nsm, float* h
   }
 }
 
+cudaError_t hash_lists(const Params& P, const DeviceIndex& di, const float* Q, int nq, const int* q_qprobes, int qp_max,
+                       float* list_v, uint32_t* list_b, long long stride, float* heap_v, int* heap_i,
+                       long long max_groups, cudaStream_t s) {
+  const int L = P.n_tables, D = P.n_proj;
+  int log2D = 0;
+  while ((1 << log2D) < D) ++log2D;
+  int dev = 0, nsm = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  QHashArgs qa;
+  qa.Q = Q;
+  qa.nq = nq;
+  qa.d = P.n_features;
+  qa.flips = di.flips;
+  qa.L = L;
+  qa.D = D;
+  qa.log2D = log2D;
+  qa.NB = 4u * (uint32_t)D * (uint32_t)D;
+  qa.m = (2 * qp_max + L - 1) / L;
+  int m1 = 0;
+  while (m1 * m1 < qa.m) ++m1;
+  qa.m1 = m1;
+  qa.list_v = list_v;
+  qa.list_b = list_b;
+  qa.q_qprobes = q_qprobes;
+  qa.qp_max = qp_max;
+  qa.stride = stride;
+  return dispatch_qhash(P.fhtDim, qa, nsm, heap_v, heap_i, max_groups, s);
+}
+
 template <typename T>
 static cudaError_t ensure(T*& p, size_t& cap_elems, size_t need) {
   if (need <= cap_elems && p) return cudaSuccess;
@@ -680,6 +727,9 @@ int query_index(const Params& P, const DeviceIndex& di, const float* Q, bool q_o
     qa.m1 = m1;
     qa.list_v = ws.list_v;
     qa.list_b = ws.list_b;
+    qa.q_qprobes = nullptr;
+    qa.qp_max = Qp;
+    qa.stride = M;
     if ((e = dispatch_qhash(F, qa, nsm, ws.heap_v, ws.heap_i, max_groups, s)) != cudaSuccess)
       return fail(e, "k_query_hash");
   }

@@ -73,6 +73,15 @@ struct QueryDumps {
   long long cand_stride = 0;
 };
 
+// The per-table probe lists of every query (rotate + hash + pair top-m,
+// src/FalconnPP.cpp:358-531) with the plain path's kernel, for the batched
+// form: q_qprobes (device, nullable: every query uses qp_max) gives each
+// query its own m; query q's lists start at list_v / list_b + q * stride.
+// heap_v / heap_i: max_groups * ceil(2 qp_max / L) scratch entries.
+cudaError_t hash_lists(const Params& P, const DeviceIndex& di, const float* Q, int nq, const int* q_qprobes, int qp_max,
+                       float* list_v, uint32_t* list_b, long long stride, float* heap_v, int* heap_i,
+                       long long max_groups, cudaStream_t s);
+
 int query_index(const Params& P, const DeviceIndex& di, const float* Q, bool q_on_device, int nq, int k,
                 int32_t* out, bool out_on_device, QueryWorkspace& ws, QueryStats& st, cudaStream_t s,
                 Error& err, QueryDumps* dumps);

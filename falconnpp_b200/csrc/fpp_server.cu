@@ -138,6 +138,7 @@ fpp::BatchRequest slot_request(const fpp_server* S, const Slot& s, int nq) {
   rq.blocks_per_sm = std::max(1, 3 / (int)S->slots.size());
   rq.reorder = h->reorder;
   rq.tc_rotation = h->tc_rotation;
+  rq.split_hash = h->split_hash;
   return rq;
 }
 
