@@ -305,6 +305,31 @@ def run_ours(args, w, rank, world, local_rank):
                                             "note": "opt-in tensor-core rotation with FP16 operands: not the "
                                                     "reference's FP32 hash, excluded from the headline"}}
 
+    # the brute-force block rerank on the tcgen05 tensor cores (every point
+    # against every query, BF16 / FP8, exact FP32 re-score of a 4k
+    # shortlist): another method, reported beside the LSF forms
+    bf = {}
+    if args.form == "all":
+        for bname, bprec in (("bruteforce-bf16", 1), ("bruteforce-fp8", 2)):
+            def bf_call():
+                idx.bruteforce_lowp(Qd.data_ptr(), nq, k, bprec, 4, outd.data_ptr(), None, sp)
+            bf_call()
+            torch.cuda.synchronize()
+            br = recall(truth, outd[:ns].cpu().numpy(), k)
+            ev0 = torch.cuda.Event(enable_timing=True)
+            ev1 = torch.cuda.Event(enable_timing=True)
+            with torch.cuda.stream(tstream):
+                ev0.record()
+                for _ in range(max(1, args.steps // 2)):
+                    bf_call()
+                ev1.record()
+            torch.cuda.synchronize()
+            bms = reduce_max(ev0.elapsed_time(ev1)) / max(1, args.steps // 2)
+            tflop = 2.0 * w["n"] * nq * d / 1e12
+            bf[bname] = {"value": round(world * nq / (bms / 1000.0), 1), "ms_per_step": round(bms, 4),
+                         "recall_at_k": round(br, 4), "tensor_tflops": round(tflop / (bms / 1000.0), 1),
+                         "shortlist": 4 * k}
+
     # headline: the fastest batched form that reaches the recall target
     cands = [f for f in forms if f != "plain-fp32" and results[f]["recall"] >= RECALL_TARGET] or forms
     head = max(cands, key=lambda f: results[f]["value"])
@@ -397,6 +422,8 @@ def run_ours(args, w, rank, world, local_rank):
     }
     if variant:
         result["variants_not_headline"] = variant
+    if bf:
+        result["bruteforce_block"] = bf
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         result["cpu_baseline"] = cpu_baseline_from_index(idx, X, Q, w, chosen)
     return result
@@ -604,6 +631,25 @@ def run_precision(args):
             r["max_abs_err_lowp_dot"] = float((lpd - exact).abs().max())
             r["max_rel_err_lowp_dot"] = float(((lpd - exact).abs() / exact.abs().clamp_min(1e-12)).max())
         forms[name] = r
+    # the brute-force block rerank on the tensor cores: every point, BF16 /
+    # FP8 with FP32 accumulation, exact FP32 re-score of a 4k shortlist
+    for name, prec in (("bruteforce-bf16", 1), ("bruteforce-fp8", 2)):
+        idx.bruteforce_lowp(Qd.data_ptr(), nq, k, prec, 4, out.data_ptr(), val.data_ptr(), stream.cuda_stream)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            e0.record()
+            for _ in range(max(1, args.steps // 2)):
+                idx.bruteforce_lowp(Qd.data_ptr(), nq, k, prec, 4, out.data_ptr(), val.data_ptr(),
+                                    stream.cuda_stream)
+            e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / max(1, args.steps // 2)
+        ids = out.cpu().numpy()
+        forms[name] = {"value": round(nq / (ms / 1000.0), 1), "ms_per_step": round(ms, 4),
+                       "recall_at_10": round(recall(truth, ids[:ns], k), 4),
+                       "tensor_tflops": round(2.0 * w["n"] * nq * w["d"] / 1e12 / (ms / 1000.0), 1)}
     return {"workload": "precision-10Mx128", "config": {k2: v for k2, v in w.items()}, "build_s": round(build_s, 2),
             "forms": forms, "data": "synthetic", "unit": "queries/s"}
 
@@ -630,7 +676,10 @@ def run_mixed(args):
     qpd = torch.from_numpy(qps).cuda()
     out = torch.zeros((len(Q), k), dtype=torch.int32, device="cuda")
     stream = torch.cuda.Stream()
-    idx.set_query_form(1, 1, 4)
+    # start from the autotuned configuration (a sample of the batch at the
+    # middle qProbes, 99 % agreement with the exact FP32 ids)
+    idx.set_qprobes(20)
+    tuned = idx.autotune(Qd.data_ptr(), 4096, k, 0.99, stream.cuda_stream)
     idx.set_option("use_graph", 1)
 
     def one_pass():
@@ -653,7 +702,7 @@ def run_mixed(args):
     return {"workload": "mixed-1Mx200", "value": round(len(Q) / (ms / 1000.0), 1), "unit": "queries/s",
             "batches": len(sizes), "ms_total": round(ms, 3), "recall_at_20": round(recall(truth, out[:ns].cpu().numpy(), k), 4),
             "config": {"queries": len(Q), "batch_sizes": "uniform 1..4096", "qprobes": "per query from {5,10,20,80}",
-                       "k": k, "form": "batched-bf16 x4 shortlist, CUDA graph"}, "data": "synthetic"}
+                       "k": k, "form": "batched, autotuned, CUDA graph", "tuned": tuned}, "data": "synthetic"}
 
 
 def run_serve(args, big=True):
@@ -676,7 +725,11 @@ def run_serve(args, big=True):
     # exact FP64 top-100 of every pool query: the top-k prefix is the exact
     # top-k (ties by ascending id), so every served query is checked
     truth = exact_topk_fp64(Xd, pool, 100)
-    idx.set_query_form(1, 1, 4)
+    import torch as _t
+    dpool = _t.from_numpy(pool[:4096]).cuda()
+    idx.set_qprobes(qp)
+    tuned = idx.autotune(dpool.data_ptr(), 4096, 10, 0.99)
+    del dpool
     results = {}
     n_requests = args.requests
     for rate in (1000, 10000, 50000, 200000):
@@ -740,7 +793,8 @@ def run_serve(args, big=True):
                               "recall_at_k": round(rec / cnt, 4) if cnt else None}
     return {"workload": "serve-10Mx128" if big else "serve-1Mx200", "rates_qps": results, "unit": "ms",
             "config": {"n": w["n"], "d": w["d"], "request_sizes": "uniform 1..1024", "k": "{1,10,100}",
-                       "qprobes": qp, "streams": 3, "form": "batched-bf16 x4", "requests_per_rate": n_requests,
+                       "qprobes": qp, "streams": 3, "form": "batched, autotuned", "tuned": tuned,
+                       "requests_per_rate": n_requests,
                        "recall": "every served query against its exact FP64 top-k"}, "data": "synthetic"}
 
 

@@ -185,11 +185,11 @@ class Index:
                                             ctypes.c_void_p(counts_ptr or 0), ctypes.c_void_p(stream or 0)))
 
     def autotune(self, q_ptr: int, nq: int, k: int, min_agreement: float = 0.99, stream: int | None = None) -> dict:
-        rep = np.zeros(6, np.float64)
+        rep = np.zeros(8, np.float64)
         _check(lib().fpp_autotune(self.h, ctypes.c_void_p(q_ptr), nq, k, min_agreement, _ptr(rep),
                                   ctypes.c_void_p(stream or 0)))
         return dict(ms=rep[0], blocks_per_sm=int(rep[1]), precision=int(rep[2]), shortlist_mult=int(rep[3]),
-                    agreement=rep[4], tried=int(rep[5]))
+                    agreement=rep[4], tried=int(rep[5]), split_hash=int(rep[6]), reorder=int(rep[7]))
 
     def bruteforce_lowp(self, q_ptr: int, nq: int, k: int, precision: int, shortlist_mult: int, out_ptr: int,
                         val_ptr: int | None = None, stream: int | None = None):

@@ -475,7 +475,7 @@ int fpp_autotune(fpp_index* h, const float* d_queries, int n_queries, int k, dou
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
   std::vector<int32_t> ref(nout), got(nout);
-  auto run = [&](int precision, int mult, int bps, int32_t* out, float* ms) -> int {
+  auto run = [&](int precision, int mult, int bps, bool split, bool reorder, int32_t* out, float* ms) -> int {
     fpp::BatchRequest rq;
     rq.Q = d_queries;
     rq.nq = n_queries;
@@ -488,9 +488,9 @@ int fpp_autotune(fpp_index* h, const float* d_queries, int n_queries, int k, dou
     rq.out = out;
     rq.out_stride = k;
     rq.blocks_per_sm = bps;
-    rq.reorder = h->reorder;
+    rq.reorder = reorder;
     rq.tc_rotation = h->tc_rotation;
-  rq.split_hash = h->split_hash;
+    rq.split_hash = split;
     rq.check_status = true;
     fpp::BatchResult res;
     fpp::Error err{0, ""};
@@ -513,9 +513,10 @@ int fpp_autotune(fpp_index* h, const float* d_queries, int n_queries, int k, dou
     return FPP_OK;
   };
   float ms = 0;
-  int rc = run(0, 1, 0, d_ref, &ms);
+  int rc = run(0, 1, 0, true, h->reorder, d_ref, &ms);
   double best_ms = 1e30, best_agree = 0;
   int best_bps = 0, best_prec = 0, best_mult = 4, tried = 0;
+  bool best_split = true, best_reorder = h->reorder;
   if (rc == FPP_OK) {
     cudaMemcpy(ref.data(), d_ref, sizeof(int32_t) * nout, cudaMemcpyDeviceToHost);
     best_ms = ms;
@@ -523,11 +524,16 @@ int fpp_autotune(fpp_index* h, const float* d_queries, int n_queries, int k, dou
     const int precs[2] = {1, 2};
     const int mults[3] = {1, 2, 4};
     const int bpss[3] = {1, 2, 3};
+    // precision x shortlist x resident blocks per SM (queries in flight per
+    // SM) x exact hash in its own kernel or inside the fused one x query
+    // grouping; the hash and grouping choices change no result
     for (int pi = 0; pi < 2 && rc == FPP_OK; ++pi)
       for (int mi = 0; mi < 3 && rc == FPP_OK; ++mi)
-        for (int bi = 0; bi < 3 && rc == FPP_OK; ++bi) {
+        for (int bi = 0; bi < 3 && rc == FPP_OK; ++bi)
+          for (int sp = 1; sp >= 0 && rc == FPP_OK; --sp)
+            for (int ro = 1; ro >= 0 && rc == FPP_OK; --ro) {
           if ((long long)k * mults[mi] > 1024) continue;
-          rc = run(precs[pi], mults[mi], bpss[bi], d_out, &ms);
+          rc = run(precs[pi], mults[mi], bpss[bi], sp != 0, ro != 0, d_out, &ms);
           if (rc) break;
           ++tried;
           cudaMemcpy(got.data(), d_out, sizeof(int32_t) * nout, cudaMemcpyDeviceToHost);
@@ -549,6 +555,8 @@ int fpp_autotune(fpp_index* h, const float* d_queries, int n_queries, int k, dou
             best_bps = bpss[bi];
             best_prec = precs[pi];
             best_mult = mults[mi];
+            best_split = sp != 0;
+            best_reorder = ro != 0;
           }
         }
   }
@@ -561,6 +569,8 @@ int fpp_autotune(fpp_index* h, const float* d_queries, int n_queries, int k, dou
   h->precision = best_prec;
   h->shortlist_mult = best_mult;
   h->blocks_per_sm = best_bps;
+  h->split_hash = best_split;
+  h->reorder = best_reorder;
   if (report) {
     report[0] = best_ms;
     report[1] = best_bps;
@@ -568,6 +578,8 @@ int fpp_autotune(fpp_index* h, const float* d_queries, int n_queries, int k, dou
     report[3] = best_mult;
     report[4] = best_agree;
     report[5] = tried;
+    report[6] = best_split ? 1 : 0;
+    report[7] = best_reorder ? 1 : 0;
   }
   return ok();
 }

@@ -188,15 +188,18 @@ int fpp_query_batched_dump(fpp_index* h, const float* d_queries, int n_queries, 
                            float* d_out_val, uint32_t* d_probes, uint32_t* d_counts, void* stream);
 
 /* Autotuner of the batched form (no reference counterpart).  On a sample of
- * device queries it times the fused kernel over blocks per SM {1,2,3},
- * precision {BF16, FP8} and shortlist multiple {1,2,4}, against the FP32
- * exact batched result (occupancy-limited blocks per SM), and keeps the
- * fastest configuration whose top-k ids agree with the exact ones on at least
+ * device queries it times the batched form over precision {BF16, FP8} x
+ * shortlist multiple {1,2,4} x resident fused blocks per SM {1,2,3} (each
+ * block works on one query at a time, so this is the queries in flight per
+ * SM) x exact hash in its own kernel or inside the fused one x query grouping
+ * on/off, against the FP32 exact batched result, and keeps the fastest
+ * configuration whose top-k ids agree with the exact ones on at least
  * min_agreement of the ids (the FP32 configuration itself when none does).
- * The handle is switched to the batched form with that configuration.
- * report (may be NULL): double[6] = best ms for the sample, blocks per SM
+ * The hash and grouping choices change no result; precision and shortlist
+ * can.  The handle is switched to the batched form with that configuration.
+ * report (may be NULL): double[8] = best ms for the sample, blocks per SM
  * (0 = occupancy limit), precision, shortlist multiple, agreement,
- * configurations tried. */
+ * configurations tried, split hash (0/1), query grouping (0/1). */
 int fpp_autotune(fpp_index* h, const float* d_queries, int n_queries, int k, double min_agreement, double* report,
                  void* stream);
 
