@@ -181,6 +181,8 @@ void BatchWorkspace::release() {
   cudaFree(gheap_v);
   cudaFree(gheap_i);
   cudaFree(counters);
+  for (auto& ev : tev)
+    if (ev) cudaEventDestroy(ev);
   cudaFree(okey);
   cudaFree(ohist);
   cudaFree(order);
@@ -336,6 +338,11 @@ int batch_query(const Params& P, DeviceIndex& di, BatchWorkspace& bw, const Batc
         return fail(e, "alloc");
       bw.hheap_cap = (long long)nh;
     }
+    if (rq.stage_timing) {
+      for (auto& ev : bw.tev)
+        if (!ev && (e = cudaEventCreate(&ev)) != cudaSuccess) return fail(e, "event create");
+      cudaEventRecord(bw.tev[0], s);
+    }
     if ((e = hash_lists(P, di, rq.Q, rq.nq, rq.q_qprobes, rq.qprobes_max, bw.ext_lv, bw.ext_lb, ext_stride,
                         bw.hheap_v, bw.hheap_i, max_groups, s)) != cudaSuccess)
       return fail(e, "hash kernel");
@@ -444,6 +451,12 @@ int batch_query(const Params& P, DeviceIndex& di, BatchWorkspace& bw, const Batc
   a.ext_stride = ext_stride;
   void* args[] = {&a};
 
+  if (rq.stage_timing) {
+    for (auto& ev : bw.tev)
+      if (!ev && (e = cudaEventCreate(&ev)) != cudaSuccess) return fail(e, "event create");
+    if (!split) cudaEventRecord(bw.tev[0], s);
+    cudaEventRecord(bw.tev[1], s);
+  }
   const bool can_graph = rq.use_graph && !rq.dump_probes && !rq.dump_counts;
   BatchKey key{rq.Q, rq.nq, rq.q_k, rq.q_qprobes, rq.k_uniform, rq.qprobes_uniform, rq.k_max, rq.qprobes_max,
                rq.shortlist_mult, rq.out,
@@ -503,6 +516,12 @@ int batch_query(const Params& P, DeviceIndex& di, BatchWorkspace& bw, const Batc
     }
   }
   res.launches = (reorder ? 3 : 1) + (split ? 1 : 0);
+  if (rq.stage_timing) {
+    cudaEventRecord(bw.tev[2], s);
+    if ((e = cudaEventSynchronize(bw.tev[2])) != cudaSuccess) return fail(e, "stage timing");
+    cudaEventElapsedTime(&res.ms_hash, bw.tev[0], bw.tev[1]);
+    cudaEventElapsedTime(&res.ms_fused, bw.tev[1], bw.tev[2]);
+  }
   res.grid = grid;
   if (rq.check_status) {
     unsigned st[2] = {0, 0};

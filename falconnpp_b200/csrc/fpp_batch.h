@@ -26,6 +26,7 @@ struct BatchRequest {
   uint32_t* dump_probes = nullptr;  // parity dumps (device, nullable; no graph): [nq][qprobes_max] probes
   uint32_t* dump_counts = nullptr;  // [nq][2] candidates, unique candidates
   bool split_hash = true;           // exact hash in its own kernel before the fused one (kHashExt)
+  bool stage_timing = false;        // CUDA events around the hash and the fused kernel (synchronises)
   bool tc_rotation = false;        // opt-in, BF16/FP8, fhtDim 256: rotate on the tensor cores (FP16 operands,
                                    // not the reference's FP32 hash: probes can differ)
 };
@@ -36,6 +37,7 @@ struct BatchResult {
   bool graph_replayed = false;
   bool overflow = false;
   bool bad_params = false;
+  float ms_hash = 0, ms_fused = 0;  // with stage_timing: the hash kernel (split form) and the fused kernel
 };
 
 struct BatchKey {
@@ -99,6 +101,7 @@ struct BatchWorkspace {
   float* hheap_v = nullptr;
   int* hheap_i = nullptr;
   long long hheap_cap = 0;
+  cudaEvent_t tev[3] = {nullptr, nullptr, nullptr};  // stage timing
   cudaGraphExec_t graph_exec = nullptr;
   cudaGraph_t graph = nullptr;
   cudaGraphNode_t graph_knode = nullptr;

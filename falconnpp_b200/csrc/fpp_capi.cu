@@ -165,6 +165,7 @@ int run_batched(fpp_index* h, const float* dQ, int nq, int k, int32_t* dout, cud
   rq.reorder = h->reorder;
   rq.tc_rotation = h->tc_rotation;
   rq.split_hash = h->split_hash;
+  rq.stage_timing = h->ws.stage_timing;
   rq.check_status = check_status;
   fpp::BatchResult res;
   fpp::Error err{0, ""};
@@ -174,6 +175,8 @@ int run_batched(fpp_index* h, const float* dQ, int nq, int k, int32_t* dout, cud
   h->qst = fpp::QueryStats();
   h->qst.launches = res.launches;
   h->qst.total_probes = (long long)nq * h->P.qProbes;
+  h->qst.ms_hash = res.ms_hash;   // with "stage_timing": the exact hash kernel (split form)
+  h->qst.ms_rerank = res.ms_fused;  // and the fused probe / gather / rerank / top-k kernel
   return FPP_OK;
 }
 
