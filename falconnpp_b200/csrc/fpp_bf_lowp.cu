@@ -55,6 +55,7 @@ constexpr int kKPadBytes = 512;     // K bytes covered (BF16: d <= 256; E4M3: d 
 constexpr int kBoxTileBytes = kTile * kBoxBytes;  // 16 KB: 128 rows of one box
 constexpr int kThreads = 192;
 constexpr int kMaxR = 256;          // shortlist per query
+constexpr int kMaxRS = 32;          // per-split heap in shared memory: 128 queries x 32 keys = 32 KB
 constexpr uint32_t kMaxPolls = 1u << 24;
 constexpr int kTmemCols = 256;
 
@@ -69,10 +70,11 @@ struct BfArgs {
   int boxes;                   // TMA boxes per tile (kbytes rounded up to 128)
   int stages;
   int rows_per_split, splits, qtiles;
-  int R;
+  int R;                       // shortlist per query (merge)
+  int rs;                      // per-split heap size, min(R, kMaxRS)
   const float* xscale;         // FP8 per-row scales (nullable for BF16)
   const float* qscale;         // FP8 per-query scales
-  unsigned long long* heap;    // [nq][splits][R] keys (ord(score) << 32) | ~id, min-heap
+  unsigned long long* heap;    // [nq][splits][rs] keys (ord(score) << 32) | ~id
   int* heap_n;                 // [nq][splits]
   unsigned* status;            // bit 0: a CTA gave up waiting
 };
@@ -170,19 +172,19 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
   for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-// size-R min-heap of keys (larger key = better candidate)
-__device__ __forceinline__ void key_heap_offer(unsigned long long* h, int& n, int R, unsigned long long key) {
+// size-R min-heap of keys (larger key = better candidate), slot j at h[j * st]
+__device__ __forceinline__ void key_heap_offer_strided(unsigned long long* h, int st, int& n, int R, unsigned long long key) {
   int i;
   if (n < R) {
     i = n++;
     while (i > 0) {
       const int p = (i - 1) >> 1;
-      const unsigned long long hp = h[p];
+      const unsigned long long hp = h[p * st];
       if (hp <= key) break;
-      h[i] = hp;
+      h[i * st] = hp;
       i = p;
     }
-    h[i] = key;
+    h[i * st] = key;
     return;
   }
   if (key <= h[0]) return;
@@ -190,19 +192,19 @@ __device__ __forceinline__ void key_heap_offer(unsigned long long* h, int& n, in
   for (;;) {
     int c = 2 * i + 1;
     if (c >= n) break;
-    unsigned long long hc = h[c];
+    unsigned long long hc = h[c * st];
     if (c + 1 < n) {
-      const unsigned long long h2 = h[c + 1];
+      const unsigned long long h2 = h[(c + 1) * st];
       if (h2 < hc) {
         hc = h2;
         ++c;
       }
     }
     if (hc >= key) break;
-    h[i] = hc;
+    h[i * st] = hc;
     i = c;
   }
-  h[i] = key;
+  h[i * st] = key;
 }
 
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
@@ -219,7 +221,8 @@ __global__ void __launch_bounds__(kThreads, 1)
   const int tile_bytes = a.boxes * kBoxTileBytes;
   unsigned char* q_smem = base;
   unsigned char* x_smem = base + tile_bytes;
-  uint64_t* bars = reinterpret_cast<uint64_t*>(x_smem + (size_t)a.stages * tile_bytes);
+  unsigned long long* heap_smem = reinterpret_cast<unsigned long long*>(x_smem + (size_t)a.stages * tile_bytes);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(heap_smem + (size_t)kTile * a.rs);
   // bars: [0] q_full, [1..S] full, [S+1..2S] empty, [2S+1..2S+2] acc full, [2S+3..2S+4] acc empty
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * a.stages + 5);
   __shared__ int s_abort;
@@ -321,7 +324,10 @@ __global__ void __launch_bounds__(kThreads, 1)
     const int ql = quad * 32 + lane;
     const int q = q0 + ql;
     const bool live = q < a.nq;
-    unsigned long long* hk = a.heap + ((size_t)(live ? q : 0) * a.splits + split) * a.R;
+    const int RS = a.rs;
+    // the split's top RS keys of this query in shared memory, slot j at
+    // hk[j * kTile] (consecutive queries in consecutive words)
+    unsigned long long* hk = heap_smem + ql;
     int hn = 0;
     float thr = -INFINITY;  // score of the heap's minimum once the heap is full
     const float qs = (MODE == kRowsFP8 && live) ? a.qscale[q] : 1.0f;
@@ -339,25 +345,48 @@ __global__ void __launch_bounds__(kThreads, 1)
       if (lane == 0) mbar_arrive(bar(2 * S + 3 + b));
       const int x0 = r0 + i * kTile;
       const int nvalid = min(kTile, r1 - x0);
-      if (live) {
 #pragma unroll
-        for (int c = 0; c < 4; ++c) {
+      for (int c = 0; c < 4; ++c) {
+        if (MODE == kRowsFP8) {
+          // lane t holds the scale of column c * 32 + t; column j's is shuffled in
+          const int xr = x0 + c * 32 + lane;
+          const float xs = xr < a.n ? __ldg(a.xscale + xr) : 0.0f;
 #pragma unroll
-          for (int j = 0; j < 32; ++j) {
-            const int col = c * 32 + j;
-            float sc = v[c][j];
-            if (MODE == kRowsFP8) sc = (sc * __ldg(a.xscale + min(x0 + col, a.n - 1))) * qs;
-            if (col < nvalid && (hn < a.R || sc >= thr)) {
-              const unsigned long long key =
-                  ((unsigned long long)ord_key(sc) << 32) | (uint32_t)~(uint32_t)(x0 + col);
-              key_heap_offer(hk, hn, a.R, key);
-              if (hn == a.R) thr = __uint_as_float(ord_key_inv_dev((uint32_t)(hk[0] >> 32)));
+          for (int jj = 0; jj < 32; ++jj) v[c][jj] = (v[c][jj] * __shfl_sync(kFullMask, xs, jj)) * qs;
+        }
+        // one compare per score: the columns at or above the heap's minimum
+        uint32_t mask = 0;
+#pragma unroll
+        for (int jj = 0; jj < 32; ++jj)
+          mask |= ((c * 32 + jj < nvalid) && (hn < RS || v[c][jj] >= thr)) ? (1u << jj) : 0u;
+        if (!live) mask = 0;
+        if (__any_sync(kFullMask, mask != 0)) {
+          // candidates: every lane takes its own next one per round, so the
+          // warp runs as many rounds as its busiest lane has candidates
+          float st[32];
+#pragma unroll
+          for (int jj = 0; jj < 32; ++jj) st[jj] = v[c][jj];
+          while (__any_sync(kFullMask, mask != 0)) {
+            if (mask) {
+              const int jj = __ffs(mask) - 1;
+              mask &= mask - 1;
+              const float sc = st[jj];
+              if (hn < RS || sc >= thr) {
+                const unsigned long long key =
+                    ((unsigned long long)ord_key(sc) << 32) | (uint32_t)~(uint32_t)(x0 + c * 32 + jj);
+                key_heap_offer_strided(hk, kTile, hn, RS, key);
+                if (hn == RS) thr = __uint_as_float(ord_key_inv_dev((uint32_t)(hk[0] >> 32)));
+              }
             }
           }
         }
       }
     }
-    if (live) a.heap_n[(size_t)q * a.splits + split] = hn;
+    if (live) {
+      unsigned long long* out = a.heap + ((size_t)q * a.splits + split) * RS;
+      for (int t = 0; t < hn; ++t) out[t] = hk[t * kTile];
+      a.heap_n[(size_t)q * a.splits + split] = hn;
+    }
   }
   __syncthreads();
   if (threadIdx.x == 0 && s_abort) atomicOr(a.status, 1u);
@@ -391,7 +420,8 @@ __device__ __forceinline__ float dot_canonical_rows(const float* q, const float*
 __global__ void __launch_bounds__(kMergeThreads) k_bf_merge(const float* __restrict__ Q, int nq, int d,
                                                             const float* __restrict__ Xc, int ld,
                                                             const unsigned long long* __restrict__ heap,
-                                                            const int* __restrict__ heap_n, int splits, int R, int k,
+                                                            const int* __restrict__ heap_n, int splits, int RS, int R,
+                                                            int k,
                                                             int32_t* __restrict__ out, float* __restrict__ out_v) {
   __shared__ unsigned long long key[kMergeMax];
   __shared__ __align__(16) float qv[1024];
@@ -408,7 +438,7 @@ __global__ void __launch_bounds__(kMergeThreads) k_bf_merge(const float* __restr
   // (score desc, then id asc)
   for (int s = 0; s < splits; ++s) {
     const int cnt = heap_n[(size_t)q * splits + s];
-    const size_t base = ((size_t)q * splits + s) * R;
+    const size_t base = ((size_t)q * splits + s) * RS;
     for (int i = tid; i < cnt; i += kMergeThreads) {
       const unsigned pos = atomicAdd(&s_n, 1u);
       key[pos] = ~heap[base + i];
@@ -578,10 +608,13 @@ extern "C" int fpp_bruteforce_topk_lowp(fpp_index* h, const float* d_queries, in
   // splits of the rows: the choice whose waves of one CTA per SM come out
   // fullest (each split keeps its own shortlist heap per query)
   const long long xtiles = (n + kTile - 1) / kTile;
-  const long long max_splits = std::min<long long>({256, xtiles, kMergeMax / R});
-  int splits = 1;
+  const long long RS = std::min<long long>(R, kMaxRS);
+  const long long max_splits = std::min<long long>({256, xtiles, kMergeMax / RS});
+  // at least R / RS splits, so the splits' heaps hold R candidates together
+  const long long min_splits = std::min<long long>(max_splits, (R + RS - 1) / RS);
+  int splits = (int)min_splits;
   double best = -1.0;
-  for (int sp = 1; sp <= max_splits; ++sp) {
+  for (int sp = (int)min_splits; sp <= max_splits; ++sp) {
     const long long ctas = (long long)qtiles * sp;
     const double waves = (double)((ctas + nsm - 1) / nsm);
     const double eff = (double)ctas / (waves * nsm);
@@ -592,7 +625,7 @@ extern "C" int fpp_bruteforce_topk_lowp(fpp_index* h, const float* d_queries, in
     if (ctas >= 8LL * nsm) break;
   }
   const long long rows_per_split = ((xtiles + splits - 1) / splits) * kTile;
-  const size_t nheap = (size_t)n_queries * splits * (size_t)R;
+  const size_t nheap = (size_t)n_queries * splits * (size_t)RS;
   if ((e = grow(scr.qrows, scr.cap_q, (size_t)qtiles * kTile * row_bytes)) ||
       (e = grow(scr.qscale, scr.cap_qs, (size_t)qtiles * kTile)) || (e = grow(scr.heap, scr.cap_hv, nheap)) ||
       (e = grow(scr.heap_n, scr.cap_n, (size_t)n_queries * splits)) ||
@@ -615,12 +648,14 @@ extern "C" int fpp_bruteforce_topk_lowp(fpp_index* h, const float* d_queries, in
   a.splits = splits;
   a.qtiles = qtiles;
   a.R = (int)R;
+  a.rs = (int)RS;
   a.xscale = h->di.Xlp_scale;
   a.qscale = scr.qscale;
   a.heap = scr.heap;
   a.heap_n = scr.heap_n;
   a.status = scr.status;
-  const size_t smem = 1024 + (size_t)(1 + a.stages) * a.boxes * kBoxTileBytes + (2 * a.stages + 5) * 8 + 16;
+  const size_t smem = 1024 + (size_t)(1 + a.stages) * a.boxes * kBoxTileBytes + (size_t)kTile * RS * 8 +
+                     (2 * a.stages + 5) * 8 + 16;
   const void* kern = precision == kRowsBF16 ? reinterpret_cast<const void*>(&k_bf_lowp<kRowsBF16>)
                                             : reinterpret_cast<const void*>(&k_bf_lowp<kRowsFP8>);
   if ((e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess)
@@ -629,7 +664,7 @@ extern "C" int fpp_bruteforce_topk_lowp(fpp_index* h, const float* d_queries, in
   void* args[] = {&qmap, &xmap, &a};
   if ((e = cudaLaunchKernel(kern, dim3((unsigned)(qtiles * splits)), dim3(kThreads), args, smem, s)) != cudaSuccess)
     return set_last_error(FPP_ERR_CUDA, std::string("bruteforce_lowp: launch: ") + cudaGetErrorString(e));
-  k_bf_merge<<<n_queries, kMergeThreads, 0, s>>>(d_queries, n_queries, d, h->di.Xc, h->di.ld, scr.heap, scr.heap_n, splits, (int)R, n_neighbors, d_out, d_out_val);
+  k_bf_merge<<<n_queries, kMergeThreads, 0, s>>>(d_queries, n_queries, d, h->di.Xc, h->di.ld, scr.heap, scr.heap_n, splits, (int)RS, (int)R, n_neighbors, d_out, d_out_val);
   unsigned st = 0;
   e = cudaMemcpyAsync(&st, scr.status, sizeof(unsigned), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
