@@ -199,6 +199,10 @@ void BatchWorkspace::release() {
   cudaFree(ext_lb);
   cudaFree(hheap_v);
   cudaFree(hheap_i);
+  cudaFree(pc_g);
+  cudaFree(pc_o);
+  cudaFree(pc_pe);
+  cudaFree(pc_n);
   *this = BatchWorkspace();
 }
 
@@ -382,6 +386,46 @@ int batch_query(const Params& P, DeviceIndex& di, BatchWorkspace& bw, const Batc
     k_order_scatter<<<1, 1024, 0, s>>>(bw.okey, rq.nq, bins, bw.ohist, bw.order);
     if ((e = cudaGetLastError()) != cudaSuccess) return fail(e, "order scatter launch");
   }
+  // split hash, small lists: the probe cut of every slot in its own kernel
+  const bool pcut = split && !big;
+  if (pcut) {
+    const long long npc = (long long)rq.nq * rq.qprobes_max;
+    if (!bw.pc_g || bw.pc_cap < npc || bw.pc_ncap < rq.nq) {
+      cudaFree(bw.pc_g);
+      cudaFree(bw.pc_o);
+      cudaFree(bw.pc_pe);
+      cudaFree(bw.pc_n);
+      bw.pc_g = bw.pc_o = bw.pc_pe = nullptr;
+      bw.pc_n = nullptr;
+      bw.pc_cap = bw.pc_ncap = 0;
+      if ((e = fpp::dev_malloc(&bw.pc_g, sizeof(uint32_t) * (size_t)npc)) != cudaSuccess ||
+          (e = fpp::dev_malloc(&bw.pc_o, sizeof(uint32_t) * (size_t)npc)) != cudaSuccess ||
+          (e = fpp::dev_malloc(&bw.pc_pe, sizeof(uint32_t) * (size_t)npc)) != cudaSuccess ||
+          (e = fpp::dev_malloc(&bw.pc_n, sizeof(int) * (size_t)rq.nq)) != cudaSuccess)
+        return fail(e, "alloc");
+      bw.pc_cap = npc;
+      bw.pc_ncap = rq.nq;
+    }
+    ProbeCutArgs pa;
+    pa.ext_lv = bw.ext_lv;
+    pa.ext_lb = bw.ext_lb;
+    pa.ext_stride = ext_stride;
+    pa.order = reorder ? bw.order : nullptr;
+    pa.q_k = rq.q_k;
+    pa.q_qprobes = rq.q_qprobes;
+    pa.k_uniform = rq.k_uniform;
+    pa.qprobes_uniform = rq.qprobes_uniform;
+    pa.k_max = rq.k_max;
+    pa.qprobes_max = rq.qprobes_max;
+    pa.L = L;
+    pa.bucket_off = di.bucket_off;
+    pa.pc_g = bw.pc_g;
+    pa.pc_o = bw.pc_o;
+    pa.pc_pe = bw.pc_pe;
+    pa.pc_n = bw.pc_n;
+    pa.stride = rq.qprobes_max;
+    if ((e = probe_cut_lists(pa, rq.nq, s)) != cudaSuccess) return fail(e, "probe cut launch");
+  }
   BatchArgs a;
   a.Xc = di.Xc;
   a.ld = di.ld;
@@ -449,6 +493,10 @@ int batch_query(const Params& P, DeviceIndex& di, BatchWorkspace& bw, const Batc
   a.ext_lv = bw.ext_lv;
   a.ext_lb = bw.ext_lb;
   a.ext_stride = ext_stride;
+  a.pc_g = pcut ? bw.pc_g : nullptr;
+  a.pc_o = pcut ? bw.pc_o : nullptr;
+  a.pc_pe = pcut ? bw.pc_pe : nullptr;
+  a.pc_n = pcut ? bw.pc_n : nullptr;
   void* args[] = {&a};
 
   if (rq.stage_timing) {
@@ -515,7 +563,7 @@ int batch_query(const Params& P, DeviceIndex& di, BatchWorkspace& bw, const Batc
         return fail(e, "launch");
     }
   }
-  res.launches = (reorder ? 3 : 1) + (split ? 1 : 0);
+  res.launches = (reorder ? 3 : 1) + (split ? 1 : 0) + (pcut ? 1 : 0);
   if (rq.stage_timing) {
     cudaEventRecord(bw.tev[2], s);
     if ((e = cudaEventSynchronize(bw.tev[2])) != cudaSuccess) return fail(e, "stage timing");

@@ -101,6 +101,12 @@ struct BatchWorkspace {
   float* hheap_v = nullptr;
   int* hheap_i = nullptr;
   long long hheap_cap = 0;
+  // split hash with small lists: k_probe_cut's output per processing slot
+  uint32_t* pc_g = nullptr;
+  uint32_t* pc_o = nullptr;
+  uint32_t* pc_pe = nullptr;
+  int* pc_n = nullptr;
+  long long pc_cap = 0, pc_ncap = 0;
   cudaEvent_t tev[3] = {nullptr, nullptr, nullptr};  // stage timing
   cudaGraphExec_t graph_exec = nullptr;
   cudaGraph_t graph = nullptr;

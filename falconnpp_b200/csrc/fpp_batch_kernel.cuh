@@ -87,7 +87,34 @@ struct BatchArgs {
   const float* ext_lv;
   const uint32_t* ext_lb;
   long long ext_stride;
+  // kHashExt with small lists: k_probe_cut's output per processing slot
+  // (slot * qprobes_max + p): probed global bucket id, bucket offset,
+  // inclusive prefix of the bucket sizes; pc_n[slot] = the slot's qProbes
+  const uint32_t* pc_g;
+  const uint32_t* pc_o;
+  const uint32_t* pc_pe;
+  const int* pc_n;
 };
+
+// Arguments of k_probe_cut (fpp_batch_ext.cu): the probe cut of the split
+// hash's per-table lists, written per processing slot.
+struct ProbeCutArgs {
+  const float* ext_lv;
+  const uint32_t* ext_lb;
+  long long ext_stride;
+  const uint32_t* order;
+  const int* q_k;
+  const int* q_qprobes;
+  int k_uniform, qprobes_uniform, k_max, qprobes_max;
+  int L;
+  const uint32_t* bucket_off;
+  uint32_t* pc_g;
+  uint32_t* pc_o;
+  uint32_t* pc_pe;
+  int* pc_n;
+  int stride;  // qprobes_max
+};
+cudaError_t probe_cut_lists(const ProbeCutArgs& a, int nq, cudaStream_t s);
 
 __device__ __forceinline__ int ceil_sqrt_int(int m) {
   int r = 0;
@@ -285,6 +312,8 @@ __global__ void __launch_bounds__(kBThreads, MODE == kRowsF32 ? 2 : 3) k_batch_q
   static_assert(HASH != kHashTC || (FHT == 256 && MODE != kRowsF32), "tensor-core rotation: fhtDim 256, BF16/FP8");
   static_assert(!(BIGL && HASH == kHashTC), "the big-list form hashes in FP32");
   constexpr int M1C = BIGL ? kBigM1 : kBMaxM1;  // per-layer list capacity
+  // the probe cut and the bucket ranges come from k_probe_cut
+  constexpr bool PCUT = HASH == kHashExt && !BIGL;
   constexpr int E = Geo<FHT>::E;
   constexpr int G = Geo<FHT>::G;
   constexpr int WORDS = Geo<FHT>::WORDS;
@@ -351,7 +380,7 @@ __global__ void __launch_bounds__(kBThreads, MODE == kRowsF32 ? 2 : 3) k_batch_q
       for (int i = tid; i < 1024; i += kBThreads) {
         const float x = i < a.d ? qv[i] : 0.0f;
         sm.q[i] = x;
-        if (i < G * E) sm.qh[(i >> 5) * kQhStride + (i & 31)] = x;
+        if (HASH != kHashExt && i < G * E) sm.qh[(i >> 5) * kQhStride + (i & 31)] = x;
         amax = fmaxf(amax, fabsf(x));
       }
       if (MODE != kRowsF32) {
@@ -458,7 +487,9 @@ __global__ void __launch_bounds__(kBThreads, MODE == kRowsF32 ? 2 : 3) k_batch_q
     // ---- 2. global top-qProbes of the L*m lists (FalconnPP.cpp:540-582):
     // rank by counting (big lists: radix selection of the qProbes-th largest
     // score); a tie straddling the cut replays the reference's heap
-    if constexpr (BIGL) {
+    if constexpr (PCUT) {
+      // k_probe_cut ranked this query's lists
+    } else if constexpr (BIGL) {
       bool tie = false;
       uint32_t t = 0;
       if (Qp < M) {
@@ -544,7 +575,7 @@ __global__ void __launch_bounds__(kBThreads, MODE == kRowsF32 ? 2 : 3) k_batch_q
       }
       __syncthreads();
     }
-    if (a.dump_probes)
+    if (!PCUT && a.dump_probes)
       for (int j = tid; j < Qp; j += kBThreads) a.dump_probes[(size_t)q * a.qprobes_max + j] = s_probe[j];
 
     // ---- 3. gather + dedupe (FalconnPP.cpp:584-606): the candidates of all
@@ -552,7 +583,20 @@ __global__ void __launch_bounds__(kBThreads, MODE == kRowsF32 ? 2 : 3) k_batch_q
     // (when a query has too many unique ids) in the block's L2 bitset
     uint32_t* s_po = BIGL ? a.gpo + (size_t)blockIdx.x * a.probe_cap : sm.po();
     uint32_t* s_pe = BIGL ? a.gpe + (size_t)blockIdx.x * a.probe_cap : sm.pe();
-    {
+    if constexpr (PCUT) {
+      // the ranges of the slot's probes, and their ids on the way to L2
+      const size_t pb = (size_t)qu * a.qprobes_max;
+      for (int p = tid; p < Qp; p += kBThreads) {
+        const uint32_t pe = a.pc_pe[pb + p];
+        const uint32_t ex = p ? a.pc_pe[pb + p - 1] : 0u;
+        const uint32_t o = a.pc_o[pb + p];
+        s_pe[p] = pe;
+        s_po[p] = o - ex;
+        if (a.dump_probes) a.dump_probes[(size_t)q * a.qprobes_max + p] = a.pc_g[pb + p];
+        const uint32_t w0 = o & ~3u, w1 = min(o + (pe - ex), w0 + 4096u) & ~3u;
+        if (w1 > w0) prefetch_l2(a.ids + w0, (w1 - w0) * 4u);
+      }
+    } else {
       long long run = 0;
       for (int base = 0; base < Qp; base += kBThreads) {
         const int p = base + tid;
@@ -901,7 +945,11 @@ __global__ void __launch_bounds__(kBThreads, MODE == kRowsF32 ? 2 : 3) k_batch_q
       __syncthreads();
     }
     // ---- 6. leave the hash set empty and the bitset clear
-    for (int i = tid; i < kHT; i += kBThreads) sm.ht[i] = kEmpty;
+    {
+      const uint4 e4 = make_uint4(kEmpty, kEmpty, kEmpty, kEmpty);
+      uint4* h4 = reinterpret_cast<uint4*>(sm.ht);
+      for (int i = tid; i < kHT / 4; i += kBThreads) h4[i] = e4;
+    }
     if (bits_dirty)
       for (unsigned i = tid; i < U; i += kBThreads) bits[uq[i] >> 5] = 0u;
   }

@@ -52,39 +52,42 @@ __device__ __forceinline__ void f32x2_fma_sign(float& y0, float& y1, float sg, f
       : "f"(sg), "f"(o0), "f"(o1));
 }
 
-// In-place FWHT of the group's vector, stages in increasing stride.
+// In-place FWHT of the group's vector, stages in increasing stride.  EL is
+// the number of elements per lane (lane gl holds elements [gl EL, gl EL + EL)):
+// Geo<FHT>::E by default, 128 for the wide query-hash kernel.
 //
-// With 32 elements per lane, elements j and j + 16 travel as one pair through
-// the packed instructions above, so every stage except h = 16 (which pairs j
-// with j + 16 itself) issues half the arithmetic instructions.
-template <int FHT>
-__device__ __forceinline__ void fwht_group(float (&y)[Geo<FHT>::E], int gl) {
-  constexpr int E = Geo<FHT>::E;
-  constexpr int G = Geo<FHT>::G;
-  if constexpr (E == 32) {
+// With 32 or more elements per lane, elements j and j + EL/2 travel as one
+// pair through the packed instructions above, so every stage except h = EL/2
+// (which pairs j with j + EL/2 itself) issues half the arithmetic instructions.
+template <int FHT, int EL = Geo<FHT>::E>
+__device__ __forceinline__ void fwht_group(float (&y)[EL], int gl) {
+  constexpr int E = EL;
+  constexpr int G = FHT / EL;
+  if constexpr (E >= 32) {
+    constexpr int HALF = E / 2;
 #pragma unroll
-    for (int h = 1; h < 16; h <<= 1) {
+    for (int h = 1; h < HALF; h <<= 1) {
 #pragma unroll
-      for (int i = 0; i < 16; i += 2 * h) {
+      for (int i = 0; i < HALF; i += 2 * h) {
 #pragma unroll
-        for (int j = i; j < i + h; ++j) f32x2_butterfly(y[j], y[j + 16], y[j + h], y[j + h + 16]);
+        for (int j = i; j < i + h; ++j) f32x2_butterfly(y[j], y[j + HALF], y[j + h], y[j + h + HALF]);
       }
     }
 #pragma unroll
-    for (int j = 0; j < 16; ++j) {
+    for (int j = 0; j < HALF; ++j) {
       const float a = y[j];
-      const float b = y[j + 16];
+      const float b = y[j + HALF];
       y[j] = __fadd_rn(a, b);
-      y[j + 16] = __fsub_rn(a, b);
+      y[j + HALF] = __fsub_rn(a, b);
     }
 #pragma unroll
     for (int s = 1; s < G; s <<= 1) {
       const float sg = (gl & s) ? -1.0f : 1.0f;
 #pragma unroll
-      for (int e = 0; e < 16; ++e) {
+      for (int e = 0; e < HALF; ++e) {
         const float o0 = __shfl_xor_sync(kFullMask, y[e], s);
-        const float o1 = __shfl_xor_sync(kFullMask, y[e + 16], s);
-        f32x2_fma_sign(y[e], y[e + 16], sg, o0, o1);
+        const float o1 = __shfl_xor_sync(kFullMask, y[e + HALF], s);
+        f32x2_fma_sign(y[e], y[e + HALF], sg, o0, o1);
       }
     }
     return;
@@ -117,24 +120,29 @@ __device__ __forceinline__ void fwht_group(float (&y)[Geo<FHT>::E], int gl) {
   }
 }
 
-// Flip the signs selected by the lane's flip word (bit e -> element e).
-template <int FHT>
-__device__ __forceinline__ void flip_signs(float (&y)[Geo<FHT>::E], uint32_t w) {
+// Flip the signs selected by the lane's flip words (bit e % 32 of word
+// e / 32 -> element e).
+template <int FHT, int EL = Geo<FHT>::E>
+__device__ __forceinline__ void flip_signs(float (&y)[EL], const uint32_t (&w)[EL >= 32 ? EL / 32 : 1]) {
 #pragma unroll
-  for (int e = 0; e < Geo<FHT>::E; ++e)
-    y[e] = __uint_as_float(__float_as_uint(y[e]) ^ (((w >> e) & 1u) << 31));
+  for (int e = 0; e < EL; ++e)
+    y[e] = __uint_as_float(__float_as_uint(y[e]) ^ (((w[e >> 5] >> (e & 31)) & 1u) << 31));
 }
 
 // Three rounds of (sign, FWHT) for one layer of one table.  `flips` points at
-// the 3 x WORDS flip words of that (layer, table).
-template <int FHT>
-__device__ __forceinline__ void hd3_rotate(float (&y)[Geo<FHT>::E], const uint32_t* flips, int gl) {
+// the 3 x WORDS flip words of that (layer, table); bit i % 32 of word i / 32
+// flips element i of the vector.
+template <int FHT, int EL = Geo<FHT>::E>
+__device__ __forceinline__ void hd3_rotate(float (&y)[EL], const uint32_t* flips, int gl) {
   constexpr int WORDS = Geo<FHT>::WORDS;
+  constexpr int NW = EL >= 32 ? EL / 32 : 1;  // flip words per lane
 #pragma unroll
   for (int r = 0; r < 3; ++r) {
-    const uint32_t w = flips[r * WORDS + (FHT < 32 ? 0 : gl)];
-    flip_signs<FHT>(y, w);
-    fwht_group<FHT>(y, gl);
+    uint32_t w[NW];
+#pragma unroll
+    for (int k = 0; k < NW; ++k) w[k] = flips[r * WORDS + (FHT < 32 ? 0 : gl * NW + k)];
+    flip_signs<FHT, EL>(y, w);
+    fwht_group<FHT, EL>(y, gl);
   }
 }
 
@@ -347,12 +355,14 @@ __device__ __forceinline__ int group_top2_cp(const float (&y)[Geo<FHT>::E], int 
 // it in place of the top-2 with the same tie replay.  Two passes: the group
 // maximum of |y| (one max per element), then the count, first position and
 // signed value of the elements equal to it.
-template <int FHT>
-__device__ __forceinline__ bool group_top1_strict(const float (&y)[Geo<FHT>::E], int gl, int D, int log2D,
+template <int FHT, int EL = Geo<FHT>::E>
+__device__ __forceinline__ bool group_top1_strict(const float (&y)[EL], int gl, int D, int log2D,
                                                   float* out_v, int* out_c) {
-  constexpr int E = Geo<FHT>::E;
-  constexpr int G = Geo<FHT>::G;
+  constexpr int E = EL;
+  constexpr int G = FHT / EL;
   const int lim = D - gl * E;  // elements of this lane that are coordinates (< D)
+  int cnt = 0, pos = 0;
+  float sy = 0.0f;
   float lm = -1.0f;
   if (lim >= E) {
 #pragma unroll
@@ -365,8 +375,6 @@ __device__ __forceinline__ bool group_top1_strict(const float (&y)[Geo<FHT>::E],
   float gm = lm;
 #pragma unroll
   for (int s = 1; s < G; s <<= 1) gm = fmaxf(gm, __shfl_xor_sync(kFullMask, gm, s));
-  int cnt = 0, pos = 0;
-  float sy = 0.0f;
 #pragma unroll
   for (int e = E - 1; e >= 0; --e) {
     const bool eq = e < lim && fabsf(y[e]) == gm;
