@@ -313,7 +313,6 @@ int fpp_set_option(fpp_index* h, const char* key, long long value) {
     h->tc_rotation = value != 0;
   } else if (!strcmp(key, "split_hash")) {
     h->split_hash = value != 0;
-
   } else if (!strcmp(key, "blocks_per_sm")) {
     if (value < 0) return fail(FPP_ERR_INVALID_ARGUMENT, "set_option: blocks_per_sm must be >= 0");
     h->blocks_per_sm = (int)value;
