@@ -735,8 +735,9 @@ def run_mixed(args):
 
 def run_serve(args, big=True):
     """Serving loop (continuous batching) on the 10M x 128 index (or the 1M x 200
-    one): Poisson arrivals at several rates, requests of 1..1,024 queries with
-    k in {1, 10, 100}; p50/p99 request latency, achieved QPS, recall@k on a sample."""
+    one): Poisson arrivals at 2k, 10k, 50k and 200k queries/s, --requests
+    requests per rate of 1..1,024 queries with k in {1, 10, 100}; p50/p99
+    request latency, achieved QPS, recall@k of every served query."""
     import threading
 
     import torch
@@ -760,7 +761,7 @@ def run_serve(args, big=True):
     del dpool
     results = {}
     n_requests = args.requests
-    for rate in (1000, 10000, 50000, 200000):
+    for rate in (2000, 10000, 50000, 200000):
         srv = capi.Server(idx, n_streams=3, memory_budget=256 << 20, max_batch=8192, k_max=100, qprobes_max=qp)
         rng = np.random.default_rng(rate)
         mean_req = 512.5

@@ -4,24 +4,33 @@
 // the shortlist (the block rerank of the precision form; model: BF::mips_topK,
 // src/BF.cpp:17-86, an exact GEMV + size-k min-heap per query).
 //
-// k_bf_lowp — one CTA per (query tile of 128, split of the rows):
-//   warp 0      TMA producer: the query tile once, then row tiles of 128 into
-//               a ring of shared-memory stages (128-byte swizzle, K-major);
+// k_bf_lowp — one persistent CTA per SM.  The (query tile of 128, row tile
+// of 128) pairs, in query-tile-major order, are cut into units of equal
+// length; CTA c takes units [c P, c P + P), a contiguous range, so every SM
+// gets the same number of MMAs.  A segment is a unit's part inside one query
+// tile; the query tile changes only between segments.
+//   warp 0      TMA producer: the query tile at each change of query tile
+//               (once the MMAs of the previous one have retired), row tiles
+//               into a ring of shared-memory stages (128-byte swizzle, K-major);
 //   warp 1      owns TMEM (256 columns: two 128-column accumulators) and
 //               issues tcgen05.mma (M = 128 queries, N = 128 rows, K = 16
 //               BF16 / 32 E4M3 per instruction, FP32 accumulate), committing
 //               each tile to the stage's "empty" and the accumulator's "full"
-//               barrier;
+//               barrier, and the last tile of a query tile to "query empty";
 //   warps 2..5  epilogue: thread = one query (TMEM lane), reads its 128
-//               scores with tcgen05.ld, applies the FP8 row/query scales and
-//               keeps its own size-R min-heap of 64-bit keys (score, ~id), so
-//               the kept set is the split's top R by (score desc, id asc)
-//               even among equal scores (global scratch, touched only on the
-//               rare insertions at or above the heap's minimum).
-// The CTAs of one split run side by side over the same rows, so a row tile
-// comes from HBM once and from L2 for the other query tiles.
+//               scores with tcgen05.ld, applies the FP8 row scales (staged in
+//               shared memory per tile), and keeps the segment's top RS keys
+//               (score, ~id) in a shared-memory heap, so the kept set is the
+//               segment's best by (score desc, id asc) even among equal
+//               scores.  A chunk of 32 columns whose maximum is below every
+//               lane's heap minimum is skipped after one max per score; the
+//               others insert their candidates in warp-synchronous rounds.
+//               At the end of a segment the heap goes to global memory.
+// Long segments keep the heaps warm (few insertions), and the query tiles
+// that read the same rows run side by side, so a row tile comes from HBM
+// about once and from L2 for the others.
 //
-// k_bf_merge — one block per query: the S heaps' candidates, the best R by
+// k_bf_merge — one block per query: the segments' candidates, the best R by
 // the low-precision score (ties: smaller id), their exact FP32 inner
 // products in the canonical dot order of the query path, and the top k by
 // (score desc, id asc).
@@ -55,7 +64,7 @@ constexpr int kKPadBytes = 512;     // K bytes covered (BF16: d <= 256; E4M3: d 
 constexpr int kBoxTileBytes = kTile * kBoxBytes;  // 16 KB: 128 rows of one box
 constexpr int kThreads = 192;
 constexpr int kMaxR = 256;          // shortlist per query
-constexpr int kMaxRS = 32;          // per-split heap in shared memory: 128 queries x 32 keys = 32 KB
+constexpr int kMaxRS = 32;          // per-segment heap in shared memory: 128 queries x 32 keys = 32 KB
 constexpr uint32_t kMaxPolls = 1u << 24;
 constexpr int kTmemCols = 256;
 
@@ -69,13 +78,16 @@ struct BfArgs {
   int n, nq, d, kbytes;        // kbytes: K bytes actually multiplied (multiple of 32)
   int boxes;                   // TMA boxes per tile (kbytes rounded up to 128)
   int stages;
-  int rows_per_split, splits, qtiles;
+  int qtiles;
+  long long xtiles;            // row tiles of 128
+  long long tiles_per_unit;    // a unit: this many consecutive (query tile, row tile) tiles
+  int units_per_cta;
+  int max_segs;                // segments of one query tile, at most
   int R;                       // shortlist per query (merge)
-  int rs;                      // per-split heap size, min(R, kMaxRS)
+  int rs;                      // per-segment heap size, min(R, kMaxRS)
   const float* xscale;         // FP8 per-row scales (nullable for BF16)
-  const float* qscale;         // FP8 per-query scales
-  unsigned long long* heap;    // [nq][splits][rs] keys (ord(score) << 32) | ~id
-  int* heap_n;                 // [nq][splits]
+  unsigned long long* heap;    // [nq][max_segs][rs] keys (ord(score) << 32) | ~id
+  int* heap_n;                 // [nq][max_segs] (zero for a segment that does not exist)
   unsigned* status;            // bit 0: a CTA gave up waiting
 };
 
@@ -211,6 +223,22 @@ __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
+// The CTA's tiles: the contiguous range [c0, c1) of the (query tile, row
+// tile) order t = qt * xtiles + xt, units_per_cta units of tiles_per_unit
+// tiles.  A segment is the part of a unit inside one query tile; each keeps
+// its own top-RS per query.
+struct TileWalk {
+  long long c0, T;
+  int ntiles;
+  __device__ TileWalk(const BfArgs& a) {
+    T = (long long)a.qtiles * a.xtiles;
+    const long long span = (long long)a.units_per_cta * a.tiles_per_unit;
+    c0 = (long long)blockIdx.x * span;
+    const long long c1 = min(T, c0 + span);
+    ntiles = c1 > c0 ? (int)(c1 - c0) : 0;
+  }
+};
+
 template <int MODE>
 __global__ void __launch_bounds__(kThreads, 1)
     k_bf_lowp(const __grid_constant__ CUtensorMap qmap, const __grid_constant__ CUtensorMap xmap, BfArgs a) {
@@ -222,34 +250,34 @@ __global__ void __launch_bounds__(kThreads, 1)
   unsigned char* q_smem = base;
   unsigned char* x_smem = base + tile_bytes;
   unsigned long long* heap_smem = reinterpret_cast<unsigned long long*>(x_smem + (size_t)a.stages * tile_bytes);
-  uint64_t* bars = reinterpret_cast<uint64_t*>(heap_smem + (size_t)kTile * a.rs);
-  // bars: [0] q_full, [1..S] full, [S+1..2S] empty, [2S+1..2S+2] acc full, [2S+3..2S+4] acc empty
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * a.stages + 5);
+  float* xs_smem = reinterpret_cast<float*>(heap_smem + (size_t)kTile * a.rs);  // FP8: 4 x 128 row scales
+  uint64_t* bars = reinterpret_cast<uint64_t*>(xs_smem + (MODE == kRowsFP8 ? 4 * kTile : 0));
+  // bars: [0..S) full, [S..2S) empty, [2S, 2S+1] acc full, [2S+2, 2S+3] acc
+  // empty, [2S+4] query tile full, [2S+5] query tile empty
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * a.stages + 6);
   __shared__ int s_abort;
 
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
   const int S = a.stages;
-  const int qt = blockIdx.x % a.qtiles;
-  const int split = blockIdx.x / a.qtiles;
-  const int q0 = qt * kTile;
-  const int r0 = split * a.rows_per_split;
-  const int r1 = min(a.n, r0 + a.rows_per_split);
-  const int ntiles = r1 > r0 ? (r1 - r0 + kTile - 1) / kTile : 0;
+  const TileWalk tw(a);
+  const int ntiles = tw.ntiles;
+  const long long xtiles = a.xtiles;
   const int ksteps = a.kbytes / 32;
-
   auto bar = [&](int i) { return smem_u32(bars + i); };
+  const int B_FULL = 0, B_EMPTY = S, B_ACCF = 2 * S, B_ACCE = 2 * S + 2, B_QF = 2 * S + 4, B_QE = 2 * S + 5;
   if (threadIdx.x == 0) {
     s_abort = 0;
-    mbar_init(bar(0), 1);
     for (int s = 0; s < S; ++s) {
-      mbar_init(bar(1 + s), 1);
-      mbar_init(bar(1 + S + s), 1);
+      mbar_init(bar(B_FULL + s), 1);
+      mbar_init(bar(B_EMPTY + s), 1);
     }
     for (int b = 0; b < 2; ++b) {
-      mbar_init(bar(2 * S + 1 + b), 1);
-      mbar_init(bar(2 * S + 3 + b), 4);  // one arrival per epilogue warp
+      mbar_init(bar(B_ACCF + b), 1);
+      mbar_init(bar(B_ACCE + b), 4);  // one arrival per epilogue warp
     }
+    mbar_init(bar(B_QF), 1);
+    mbar_init(bar(B_QE), 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
@@ -265,75 +293,108 @@ __global__ void __launch_bounds__(kThreads, 1)
   volatile int* abort_flag = &s_abort;
 
   if (warp == 0) {
-    // ---- producer
+    // ---- producer: a query tile at each change of query tile (once the
+    // MMAs of the previous one are done), row tiles into the stage ring
     if (lane == 0) {
-      int issued = 0;
+      int issued = 0, qloads = 0;
       bool ok = true;
-      mbar_expect_tx(bar(0), (uint32_t)tile_bytes);
-      for (int bx = 0; bx < a.boxes; ++bx)
-        tma_load_2d(smem_u32(q_smem + bx * kBoxTileBytes), &qmap, bx * C::box_elems, q0, bar(0));
       for (int i = 0; i < ntiles && ok; ++i) {
+        const long long t = tw.c0 + i;
+        const long long qt = t / xtiles;
+        const long long xt = t - qt * xtiles;
+        if (i == 0 || xt == 0) {
+          if (qloads > 0) ok = mbar_wait(bar(B_QE), (qloads - 1) & 1, abort_flag);
+          if (!ok) break;
+          mbar_expect_tx(bar(B_QF), (uint32_t)tile_bytes);
+          for (int bx = 0; bx < a.boxes; ++bx)
+            tma_load_2d(smem_u32(q_smem + bx * kBoxTileBytes), &qmap, bx * C::box_elems, (int)(qt * kTile), bar(B_QF));
+          ++qloads;
+        }
         const int s = i % S;
-        ok = mbar_wait(bar(1 + S + s), ((i / S) & 1) ^ 1, abort_flag);
+        ok = mbar_wait(bar(B_EMPTY + s), ((i / S) & 1) ^ 1, abort_flag);
         if (!ok) break;
-        mbar_expect_tx(bar(1 + s), (uint32_t)tile_bytes);
+        mbar_expect_tx(bar(B_FULL + s), (uint32_t)tile_bytes);
         unsigned char* dst = x_smem + (size_t)s * tile_bytes;
         for (int bx = 0; bx < a.boxes; ++bx)
-          tma_load_2d(smem_u32(dst + bx * kBoxTileBytes), &xmap, bx * C::box_elems, r0 + i * kTile, bar(1 + s));
+          tma_load_2d(smem_u32(dst + bx * kBoxTileBytes), &xmap, bx * C::box_elems, (int)(xt * kTile), bar(B_FULL + s));
         issued = i + 1;
       }
       // let every copy issued land before the CTA can exit (bounded)
-      mbar_wait(bar(0), 0, abort_flag);
-      for (int i = max(0, issued - S); i < issued; ++i) {
-        volatile int never = 0;
-        mbar_wait(bar(1 + i % S), (i / S) & 1, &never);
-      }
+      volatile int never = 0;
+      if (qloads > 0) mbar_wait(bar(B_QF), (qloads - 1) & 1, &never);
+      for (int i = max(0, issued - S); i < issued; ++i) mbar_wait(bar(B_FULL + i % S), (i / S) & 1, &never);
     }
   } else if (warp == 1) {
     // ---- MMA issuer
     if (lane == 0) {
-      bool ok = mbar_wait(bar(0), 0, abort_flag);
       const uint32_t qa = smem_u32(q_smem);
-      int issued = 0;
+      int issued = 0, qruns = 0;
+      bool ok = true;
       for (int i = 0; i < ntiles && ok; ++i) {
+        const long long t = tw.c0 + i;
+        const long long xt = t % xtiles;
+        if (i == 0 || xt == 0) {
+          ok = mbar_wait(bar(B_QF), qruns & 1, abort_flag);
+          if (!ok) break;
+          ++qruns;
+        }
         const int s = i % S;
         const int b = i & 1;
-        ok = mbar_wait(bar(2 * S + 3 + b), ((i >> 1) & 1) ^ 1, abort_flag);
+        ok = mbar_wait(bar(B_ACCE + b), ((i >> 1) & 1) ^ 1, abort_flag);
         if (!ok) break;
-        ok = mbar_wait(bar(1 + s), (i / S) & 1, abort_flag);
+        ok = mbar_wait(bar(B_FULL + s), (i / S) & 1, abort_flag);
         if (!ok) break;
         tc_fence_after();
         const uint32_t xa = smem_u32(x_smem + (size_t)s * tile_bytes);
-        for (int t = 0; t < ksteps; ++t) {
-          const uint32_t off = (uint32_t)((t >> 2) * kBoxTileBytes + (t & 3) * 32);
+        for (int k = 0; k < ksteps; ++k) {
+          const uint32_t off = (uint32_t)((k >> 2) * kBoxTileBytes + (k & 3) * 32);
           umma<MODE>(tmem + (uint32_t)(b * kTile), umma_desc_sw128(qa + off), umma_desc_sw128(xa + off),
-                     t > 0 ? 1u : 0u);
+                     k > 0 ? 1u : 0u);
         }
-        umma_commit(bar(1 + S + s));
-        umma_commit(bar(2 * S + 1 + b));
+        umma_commit(bar(B_EMPTY + s));
+        umma_commit(bar(B_ACCF + b));
+        // the last tile of this query tile: its MMAs release the query tile
+        if (i + 1 < ntiles && (t + 1) % xtiles == 0) umma_commit(bar(B_QE));
         issued = i + 1;
       }
       if (issued > 0) {  // the last tile's MMAs complete before TMEM is freed
         volatile int never = 0;
-        mbar_wait(bar(2 * S + 1 + ((issued - 1) & 1)), ((issued - 1) >> 1) & 1, &never);
+        mbar_wait(bar(B_ACCF + ((issued - 1) & 1)), ((issued - 1) >> 1) & 1, &never);
       }
     }
   } else {
-    // ---- epilogue: thread = query q of the tile
+    // ---- epilogue: thread = query of the tile (TMEM lane)
     const int quad = warp & 3;  // the TMEM lanes this warp may read
     const int ql = quad * 32 + lane;
-    const int q = q0 + ql;
-    const bool live = q < a.nq;
     const int RS = a.rs;
-    // the split's top RS keys of this query in shared memory, slot j at
+    // the segment's top RS keys of this query in shared memory, slot j at
     // hk[j * kTile] (consecutive queries in consecutive words)
     unsigned long long* hk = heap_smem + ql;
+    float* xs_w = xs_smem + (warp - 2) * kTile;  // FP8: this warp's copy of the tile's row scales
     int hn = 0;
     float thr = -INFINITY;  // score of the heap's minimum once the heap is full
-    const float qs = (MODE == kRowsFP8 && live) ? a.qscale[q] : 1.0f;
     for (int i = 0; i < ntiles; ++i) {
+      const long long t = tw.c0 + i;
+      const long long qt = t / xtiles;
+      const long long xt = t - qt * xtiles;
+      const int q = (int)(qt * kTile) + ql;
+      const bool live = q < a.nq;
+      const int x0 = (int)(xt * kTile);
+      const int nvalid = min(kTile, a.n - x0);
       const int b = i & 1;
-      if (!mbar_wait(bar(2 * S + 1 + b), (i >> 1) & 1, abort_flag)) break;
+      float4 xs4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+      if (MODE == kRowsFP8) {  // this tile's scales, loaded before the wait
+        const int xr = x0 + 4 * lane;
+        if (xr + 3 < a.n) {
+          xs4 = __ldg(reinterpret_cast<const float4*>(a.xscale + xr));
+        } else {
+          if (xr < a.n) xs4.x = __ldg(a.xscale + xr);
+          if (xr + 1 < a.n) xs4.y = __ldg(a.xscale + xr + 1);
+          if (xr + 2 < a.n) xs4.z = __ldg(a.xscale + xr + 2);
+        }
+      }
+      // warp-uniform: the loads and votes below need every lane
+      if (!__all_sync(kFullMask, mbar_wait(bar(B_ACCF + b), (i >> 1) & 1, abort_flag))) break;
       tc_fence_after();
       float v[4][32];
       const uint32_t taddr = tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(b * kTile);
@@ -342,50 +403,76 @@ __global__ void __launch_bounds__(kThreads, 1)
       tmem_wait_ld();
       tc_fence_before();
       __syncwarp();
-      if (lane == 0) mbar_arrive(bar(2 * S + 3 + b));
-      const int x0 = r0 + i * kTile;
-      const int nvalid = min(kTile, r1 - x0);
+      if (lane == 0) mbar_arrive(bar(B_ACCE + b));
+      if (MODE == kRowsFP8) {
+        reinterpret_cast<float4*>(xs_w)[lane] = xs4;
+        __syncwarp();
+      }
 #pragma unroll
       for (int c = 0; c < 4; ++c) {
         if (MODE == kRowsFP8) {
-          // lane t holds the scale of column c * 32 + t; column j's is shuffled in
-          const int xr = x0 + c * 32 + lane;
-          const float xs = xr < a.n ? __ldg(a.xscale + xr) : 0.0f;
+          // column j's row scale (the query's scale is one positive factor for
+          // all of its keys, so it is left out of the ordering)
 #pragma unroll
-          for (int jj = 0; jj < 32; ++jj) v[c][jj] = (v[c][jj] * __shfl_sync(kFullMask, xs, jj)) * qs;
+          for (int j4 = 0; j4 < 8; ++j4) {
+            const float4 s4 = reinterpret_cast<const float4*>(xs_w)[c * 8 + j4];
+            v[c][4 * j4] *= s4.x;
+            v[c][4 * j4 + 1] *= s4.y;
+            v[c][4 * j4 + 2] *= s4.z;
+            v[c][4 * j4 + 3] *= s4.w;
+          }
         }
-        // one compare per score: the columns at or above the heap's minimum
+        // the chunk's maximum: no column can enter a full heap below it
+        float m0 = fmaxf(v[c][0], v[c][1]), m1 = fmaxf(v[c][2], v[c][3]);
+        float m2 = fmaxf(v[c][4], v[c][5]), m3 = fmaxf(v[c][6], v[c][7]);
+#pragma unroll
+        for (int jj = 8; jj < 32; jj += 4) {
+          m0 = fmaxf(m0, v[c][jj]);
+          m1 = fmaxf(m1, v[c][jj + 1]);
+          m2 = fmaxf(m2, v[c][jj + 2]);
+          m3 = fmaxf(m3, v[c][jj + 3]);
+        }
+        const float m = fmaxf(fmaxf(m0, m1), fmaxf(m2, m3));
+        const bool cand = live && (hn < RS || m >= thr);
+        if (!__any_sync(kFullMask, cand)) continue;
+        // candidates: the columns at or above the heap's minimum
         uint32_t mask = 0;
 #pragma unroll
         for (int jj = 0; jj < 32; ++jj)
           mask |= ((c * 32 + jj < nvalid) && (hn < RS || v[c][jj] >= thr)) ? (1u << jj) : 0u;
-        if (!live) mask = 0;
-        if (__any_sync(kFullMask, mask != 0)) {
-          // candidates: every lane takes its own next one per round, so the
-          // warp runs as many rounds as its busiest lane has candidates
-          float st[32];
+        if (!cand) mask = 0;
+        // every lane takes its own next candidate per round, so the warp runs
+        // as many rounds as its busiest lane has candidates
+        float st[32];
 #pragma unroll
-          for (int jj = 0; jj < 32; ++jj) st[jj] = v[c][jj];
-          while (__any_sync(kFullMask, mask != 0)) {
-            if (mask) {
-              const int jj = __ffs(mask) - 1;
-              mask &= mask - 1;
-              const float sc = st[jj];
-              if (hn < RS || sc >= thr) {
-                const unsigned long long key =
-                    ((unsigned long long)ord_key(sc) << 32) | (uint32_t)~(uint32_t)(x0 + c * 32 + jj);
-                key_heap_offer_strided(hk, kTile, hn, RS, key);
-                if (hn == RS) thr = __uint_as_float(ord_key_inv_dev((uint32_t)(hk[0] >> 32)));
-              }
+        for (int jj = 0; jj < 32; ++jj) st[jj] = v[c][jj];
+        while (__any_sync(kFullMask, mask != 0)) {
+          if (mask) {
+            const int jj = __ffs(mask) - 1;
+            mask &= mask - 1;
+            const float sc = st[jj];
+            if (hn < RS || sc >= thr) {
+              const unsigned long long key =
+                  ((unsigned long long)ord_key(sc) << 32) | (uint32_t)~(uint32_t)(x0 + c * 32 + jj);
+              key_heap_offer_strided(hk, kTile, hn, RS, key);
+              if (hn == RS) thr = __uint_as_float(ord_key_inv_dev((uint32_t)(hk[0] >> 32)));
             }
           }
         }
       }
-    }
-    if (live) {
-      unsigned long long* out = a.heap + ((size_t)q * a.splits + split) * RS;
-      for (int t = 0; t < hn; ++t) out[t] = hk[t * kTile];
-      a.heap_n[(size_t)q * a.splits + split] = hn;
+      // the segment ends with this tile: its keys out, the heap emptied
+      const bool seg_end = (i + 1 == ntiles) || ((t + 1) % xtiles == 0) || ((t + 1) % a.tiles_per_unit == 0);
+      if (seg_end) {
+        if (live) {
+          const int seg = (int)(t / a.tiles_per_unit - (qt * xtiles) / a.tiles_per_unit);
+          unsigned long long* out = a.heap + ((size_t)q * a.max_segs + seg) * RS;
+          for (int j = 0; j < hn; ++j) out[j] = hk[j * kTile];
+          a.heap_n[(size_t)q * a.max_segs + seg] = hn;
+        }
+        hn = 0;
+        thr = -INFINITY;
+      }
+      if (MODE == kRowsFP8) __syncwarp();  // the scales are rewritten by the next tile
     }
   }
   __syncthreads();
@@ -398,7 +485,7 @@ __global__ void __launch_bounds__(kThreads, 1)
 
 // ---------------------------------------------------------------- merge + exact re-score
 constexpr int kMergeThreads = 256;
-constexpr int kMergeMax = 4096;  // splits * R candidates per query
+constexpr int kMergeMax = 4096;  // segments * RS candidates per query
 
 __device__ __forceinline__ float dot_canonical_rows(const float* q, const float* row, int nchunk, int lane) {
   float acc = 0.0f;
@@ -420,7 +507,7 @@ __device__ __forceinline__ float dot_canonical_rows(const float* q, const float*
 __global__ void __launch_bounds__(kMergeThreads) k_bf_merge(const float* __restrict__ Q, int nq, int d,
                                                             const float* __restrict__ Xc, int ld,
                                                             const unsigned long long* __restrict__ heap,
-                                                            const int* __restrict__ heap_n, int splits, int RS, int R,
+                                                            const int* __restrict__ heap_n, int segs, int RS, int R,
                                                             int k,
                                                             int32_t* __restrict__ out, float* __restrict__ out_v) {
   __shared__ unsigned long long key[kMergeMax];
@@ -434,11 +521,11 @@ __global__ void __launch_bounds__(kMergeThreads) k_bf_merge(const float* __restr
   const int nchunk = (d + 3) / 4;
   for (int i = tid; i < 4 * nchunk; i += kMergeThreads) qv[i] = i < d ? Q[(size_t)q * d + i] : 0.0f;
   __syncthreads();
-  // candidates of every split, complemented keys: ascending = best first
+  // candidates of every segment, complemented keys: ascending = best first
   // (score desc, then id asc)
-  for (int s = 0; s < splits; ++s) {
-    const int cnt = heap_n[(size_t)q * splits + s];
-    const size_t base = ((size_t)q * splits + s) * RS;
+  for (int s = 0; s < segs; ++s) {
+    const int cnt = heap_n[(size_t)q * segs + s];
+    const size_t base = ((size_t)q * segs + s) * RS;
     for (int i = tid; i < cnt; i += kMergeThreads) {
       const unsigned pos = atomicAdd(&s_n, 1u);
       key[pos] = ~heap[base + i];
@@ -605,33 +692,32 @@ extern "C" int fpp_bruteforce_topk_lowp(fpp_index* h, const float* d_queries, in
   int nsm = 148;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device);
   const int qtiles = (n_queries + kTile - 1) / kTile;
-  // splits of the rows: the choice whose waves of one CTA per SM come out
-  // fullest (each split keeps its own shortlist heap per query)
+  // one CTA per SM over the (query tile, row tile) order, in units of equal
+  // length; each unit's part in one query tile (a segment) keeps its own
+  // top-RS per query.  Units are at most xtiles / ceil(R / RS) tiles long, so
+  // a query tile has at least ceil(R / RS) segments and R candidates fit.
   const long long xtiles = (n + kTile - 1) / kTile;
+  const long long T = (long long)qtiles * xtiles;
   const long long RS = std::min<long long>(R, kMaxRS);
-  const long long max_splits = std::min<long long>({256, xtiles, kMergeMax / RS});
-  // at least R / RS splits, so the splits' heaps hold R candidates together
-  const long long min_splits = std::min<long long>(max_splits, (R + RS - 1) / RS);
-  int splits = (int)min_splits;
-  double best = -1.0;
-  for (int sp = (int)min_splits; sp <= max_splits; ++sp) {
-    const long long ctas = (long long)qtiles * sp;
-    const double waves = (double)((ctas + nsm - 1) / nsm);
-    const double eff = (double)ctas / (waves * nsm);
-    if (eff > best + 1e-9) {
-      best = eff;
-      splits = sp;
-    }
-    if (ctas >= 8LL * nsm) break;
-  }
-  const long long rows_per_split = ((xtiles + splits - 1) / splits) * kTile;
-  const size_t nheap = (size_t)n_queries * splits * (size_t)RS;
+  const long long need = (R + RS - 1) / RS;
+  const long long tu_max = std::max<long long>(1, xtiles / need);
+  // P units per CTA, then the unit length that spreads the tiles over nsm x P
+  // units: every SM gets the same work
+  const long long per_cta = std::max<long long>(1, (T + (long long)nsm * tu_max - 1) / ((long long)nsm * tu_max));
+  const long long tu = std::max<long long>(1, (T + (long long)nsm * per_cta - 1) / ((long long)nsm * per_cta));
+  const long long units = (T + tu - 1) / tu;
+  const long long grid = (units + per_cta - 1) / per_cta;
+  const long long max_segs = (xtiles + tu - 1) / tu + 1;
+  if (max_segs * RS > kMergeMax)
+    return set_last_error(FPP_ERR_UNSUPPORTED, "bruteforce_lowp: too many row segments per query tile");
+  const size_t nheap = (size_t)n_queries * max_segs * (size_t)RS;
   if ((e = grow(scr.qrows, scr.cap_q, (size_t)qtiles * kTile * row_bytes)) ||
       (e = grow(scr.qscale, scr.cap_qs, (size_t)qtiles * kTile)) || (e = grow(scr.heap, scr.cap_hv, nheap)) ||
-      (e = grow(scr.heap_n, scr.cap_n, (size_t)n_queries * splits)) ||
+      (e = grow(scr.heap_n, scr.cap_n, (size_t)n_queries * max_segs)) ||
       (!scr.status && (e = dev_malloc(&scr.status, sizeof(unsigned)))))
     return set_last_error(e == cudaErrorMemoryAllocation ? FPP_ERR_OUT_OF_MEMORY : FPP_ERR_CUDA,
                           std::string("bruteforce_lowp: ") + cudaGetErrorString(e));
+  cudaMemsetAsync(scr.heap_n, 0, sizeof(int) * (size_t)n_queries * max_segs, s);
   k_bf_queries<<<n_queries, 32, 0, s>>>(d_queries, n_queries, d, ldo, precision, scr.qrows, scr.qscale);
   CUtensorMap qmap, xmap;
   if (!make_map(&qmap, scr.qrows, (long long)n_queries, ldo, row_bytes, esize) ||
@@ -644,27 +730,29 @@ extern "C" int fpp_bruteforce_topk_lowp(fpp_index* h, const float* d_queries, in
   a.kbytes = ((d * esize + 31) / 32) * 32;
   a.boxes = (a.kbytes + kBoxBytes - 1) / kBoxBytes;
   a.stages = a.boxes <= 2 ? 4 : 2;  // 160 KB (32 KB tiles) or at most 192 KB of shared memory
-  a.rows_per_split = (int)rows_per_split;
-  a.splits = splits;
   a.qtiles = qtiles;
+  a.xtiles = xtiles;
+  a.tiles_per_unit = tu;
+  a.units_per_cta = (int)per_cta;
+  a.max_segs = (int)max_segs;
   a.R = (int)R;
   a.rs = (int)RS;
   a.xscale = h->di.Xlp_scale;
-  a.qscale = scr.qscale;
   a.heap = scr.heap;
   a.heap_n = scr.heap_n;
   a.status = scr.status;
   const size_t smem = 1024 + (size_t)(1 + a.stages) * a.boxes * kBoxTileBytes + (size_t)kTile * RS * 8 +
-                     (2 * a.stages + 5) * 8 + 16;
+                     (precision == kRowsFP8 ? 4 * kTile * 4 : 0) + (2 * a.stages + 6) * 8 + 16;
   const void* kern = precision == kRowsBF16 ? reinterpret_cast<const void*>(&k_bf_lowp<kRowsBF16>)
                                             : reinterpret_cast<const void*>(&k_bf_lowp<kRowsFP8>);
   if ((e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess)
     return set_last_error(FPP_ERR_CUDA, std::string("bruteforce_lowp: smem attribute: ") + cudaGetErrorString(e));
   cudaMemsetAsync(scr.status, 0, sizeof(unsigned), s);
   void* args[] = {&qmap, &xmap, &a};
-  if ((e = cudaLaunchKernel(kern, dim3((unsigned)(qtiles * splits)), dim3(kThreads), args, smem, s)) != cudaSuccess)
+  if ((e = cudaLaunchKernel(kern, dim3((unsigned)grid), dim3(kThreads), args, smem, s)) != cudaSuccess)
     return set_last_error(FPP_ERR_CUDA, std::string("bruteforce_lowp: launch: ") + cudaGetErrorString(e));
-  k_bf_merge<<<n_queries, kMergeThreads, 0, s>>>(d_queries, n_queries, d, h->di.Xc, h->di.ld, scr.heap, scr.heap_n, splits, (int)RS, (int)R, n_neighbors, d_out, d_out_val);
+  k_bf_merge<<<n_queries, kMergeThreads, 0, s>>>(d_queries, n_queries, d, h->di.Xc, h->di.ld, scr.heap, scr.heap_n,
+                                                 (int)max_segs, (int)RS, (int)R, n_neighbors, d_out, d_out_val);
   unsigned st = 0;
   e = cudaMemcpyAsync(&st, scr.status, sizeof(unsigned), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);

@@ -12,6 +12,9 @@ BF::mips_topK, src/BF.cpp:17-86).
   (bit-identical to the query path's dot), and repeated calls agree.
 * Ragged shapes: point and query counts that are not multiples of the
   128-row tiles.
+* Crowded neighbours: points stored in increasing order of their inner
+  product with one query, so that query's best rows all sit in the last row
+  tile (one segment holds them all), with several query tiles per CTA range.
 """
 import numpy as np
 import pytest
@@ -93,6 +96,22 @@ def test_ragged_shapes(precision):
     ref, _ = _fp64(X, Q, 5)
     assert synth.recall_at_k(ref, ids, 5) >= 0.99
     assert ids.min() >= 0 and ids.max() < X.shape[0]
+    g.close()
+
+
+@pytest.mark.parametrize("precision", [1, 2])
+def test_crowded_neighbours(precision):
+    X = synth.mixture(30000, 64, n_centres=16, seed=0)
+    Q = synth.mixture(300, 64, n_centres=16, seed=1)
+    X = np.ascontiguousarray(X[np.argsort(X @ Q[0], kind="stable")])
+    g = _index(X)
+    ids, val = _lowp(g, Q, 10, precision, 4)
+    ref, _ = _fp64(X, Q, 10)
+    assert synth.recall_at_k(ref, ids, 10) >= 0.99
+    # query 0's top 10 are the last ten ids, in one row tile
+    assert set(ref[0]) <= set(range(len(X) - 128, len(X)))
+    assert synth.recall_at_k(ref[:1], ids[:1], 10) >= 0.9
+    assert np.all(np.diff(val, axis=1) <= 0)
     g.close()
 
 
