@@ -269,7 +269,7 @@ def run_ours(args, w, rank, world, local_rank):
             # latency per step and the kernels' own durations (CUDA events on the
             # launching stream around each kernel), one step at a time
             idx.set_option("stage_timing", 1)
-            step_ms, rerank_ms, hash_ms, uniq, cand = [], [], [], 0.0, 0.0
+            step_ms, rerank_ms, hash_ms, prep_ms, uniq, cand = [], [], [], [], 0.0, 0.0
             with torch.cuda.stream(tstream):
                 for _ in range(args.steps):
                     e0 = torch.cuda.Event(enable_timing=True)
@@ -281,6 +281,7 @@ def run_ours(args, w, rank, world, local_rank):
                     step_ms.append(e0.elapsed_time(e1))
                     st = idx.stats(1)
                     hash_ms.append(st[7])
+                    prep_ms.append(st[8])
                     rerank_ms.append(st[9])
                     uniq += st[1]
                     cand += st[0]
@@ -288,7 +289,7 @@ def run_ours(args, w, rank, world, local_rank):
             idx.set_option("stage_timing", 0)
             results[fname] = dict(value=aggregate_qps(world, nq, args.steps, total_ms), ms=total_ms / args.steps,
                                   step_ms=step_ms, launches=launches, recall=r, rerank_ms=rerank_ms,
-                                  hash_ms=hash_ms)
+                                  hash_ms=hash_ms, prep_ms=prep_ms)
             if form == 0:
                 plain_stats = (uniq / args.steps, cand / args.steps, statistics.mean(rerank_ms) / 1000.0)
     # opt-in variant, not the headline: FP8 with the tensor-core rotation
@@ -411,6 +412,7 @@ def run_ours(args, w, rank, world, local_rank):
                        "add_sub_per_launch": adds, "achieved_tadds": round(adds / (hms / 1000.0) / 1e12, 2),
                        "peak_tadds": round(peak_adds, 2), "peak_kind": "nominal 148 SMs x 128 FP32 lanes x SM clock",
                        "frac": round(adds / (hms / 1000.0) / 1e12 / peak_adds, 4),
+                       "order_and_probe_cut_ms": round(statistics.mean(hr["prep_ms"]), 4),
                        "fused_kernel_ms": round(launch_s * 1e3, 4)}
     result = {
         "metric": METRIC,

@@ -350,6 +350,7 @@ int batch_query(const Params& P, DeviceIndex& di, BatchWorkspace& bw, const Batc
     if ((e = hash_lists(P, di, rq.Q, rq.nq, rq.q_qprobes, rq.qprobes_max, bw.ext_lv, bw.ext_lb, ext_stride,
                         bw.hheap_v, bw.hheap_i, max_groups, s)) != cudaSuccess)
       return fail(e, "hash kernel");
+    if (rq.stage_timing) cudaEventRecord(bw.tev[3], s);
   }
   // query order (worth it once the batch is a few waves of blocks)
   int log2D = 0;
@@ -502,7 +503,10 @@ int batch_query(const Params& P, DeviceIndex& di, BatchWorkspace& bw, const Batc
   if (rq.stage_timing) {
     for (auto& ev : bw.tev)
       if (!ev && (e = cudaEventCreate(&ev)) != cudaSuccess) return fail(e, "event create");
-    if (!split) cudaEventRecord(bw.tev[0], s);
+    if (!split) {
+      cudaEventRecord(bw.tev[0], s);
+      cudaEventRecord(bw.tev[3], s);
+    }
     cudaEventRecord(bw.tev[1], s);
   }
   const bool can_graph = rq.use_graph && !rq.dump_probes && !rq.dump_counts;
@@ -567,7 +571,8 @@ int batch_query(const Params& P, DeviceIndex& di, BatchWorkspace& bw, const Batc
   if (rq.stage_timing) {
     cudaEventRecord(bw.tev[2], s);
     if ((e = cudaEventSynchronize(bw.tev[2])) != cudaSuccess) return fail(e, "stage timing");
-    cudaEventElapsedTime(&res.ms_hash, bw.tev[0], bw.tev[1]);
+    cudaEventElapsedTime(&res.ms_hash, bw.tev[0], bw.tev[3]);
+    cudaEventElapsedTime(&res.ms_prep, bw.tev[3], bw.tev[1]);
     cudaEventElapsedTime(&res.ms_fused, bw.tev[1], bw.tev[2]);
   }
   res.grid = grid;

@@ -37,7 +37,9 @@ struct BatchResult {
   bool graph_replayed = false;
   bool overflow = false;
   bool bad_params = false;
-  float ms_hash = 0, ms_fused = 0;  // with stage_timing: the hash kernel (split form) and the fused kernel
+  // with stage_timing: the hash kernel (split form), the order and probe-cut
+  // kernels, and the fused kernel
+  float ms_hash = 0, ms_prep = 0, ms_fused = 0;
 };
 
 struct BatchKey {
@@ -107,7 +109,7 @@ struct BatchWorkspace {
   uint32_t* pc_pe = nullptr;
   int* pc_n = nullptr;
   long long pc_cap = 0, pc_ncap = 0;
-  cudaEvent_t tev[3] = {nullptr, nullptr, nullptr};  // stage timing
+  cudaEvent_t tev[4] = {nullptr, nullptr, nullptr, nullptr};  // stage timing: start, fused start, end, hash end
   cudaGraphExec_t graph_exec = nullptr;
   cudaGraph_t graph = nullptr;
   cudaGraphNode_t graph_knode = nullptr;

@@ -175,8 +175,9 @@ int run_batched(fpp_index* h, const float* dQ, int nq, int k, int32_t* dout, cud
   h->qst = fpp::QueryStats();
   h->qst.launches = res.launches;
   h->qst.total_probes = (long long)nq * h->P.qProbes;
-  h->qst.ms_hash = res.ms_hash;   // with "stage_timing": the exact hash kernel (split form)
-  h->qst.ms_rerank = res.ms_fused;  // and the fused probe / gather / rerank / top-k kernel
+  h->qst.ms_hash = res.ms_hash;     // with "stage_timing": the exact hash kernel (split form),
+  h->qst.ms_select = res.ms_prep;   // the order and probe-cut kernels,
+  h->qst.ms_rerank = res.ms_fused;  // and the fused gather / rerank / top-k kernel
   return FPP_OK;
 }
 

@@ -96,7 +96,8 @@ int fpp_get_info(fpp_index* h, long long* out, int n);
  *        probe-cut replays, top-k replays (all summed over the queries),
  *        kernels launched, then (with the "stage_timing" option) the CUDA-event
  *        milliseconds of the hashing, probe-selection and gather/rerank kernels
- *        (batched form: the exact hash kernel, 0, and the fused kernel). */
+ *        (batched form: the exact hash kernel, the order and probe-cut
+ *        kernels, and the fused kernel). */
 int fpp_get_stats(fpp_index* h, int kind, double* out, int n);
 
 /* Tuning and test switches: "exact_bucket_order" (default 1: bucket contents
