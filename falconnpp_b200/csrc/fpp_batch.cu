@@ -387,7 +387,7 @@ int batch_query(const Params& P, DeviceIndex& di, BatchWorkspace& bw, const Batc
     k_order_scatter<<<1, 1024, 0, s>>>(bw.okey, rq.nq, bins, bw.ohist, bw.order);
     if ((e = cudaGetLastError()) != cudaSuccess) return fail(e, "order scatter launch");
   }
-  // split hash, small lists: the probe cut of every slot in its own kernel
+  // split hash, small lists: the probe cut of every query in its own kernel
   const bool pcut = split && !big;
   if (pcut) {
     const long long npc = (long long)rq.nq * rq.qprobes_max;
@@ -411,7 +411,6 @@ int batch_query(const Params& P, DeviceIndex& di, BatchWorkspace& bw, const Batc
     pa.ext_lv = bw.ext_lv;
     pa.ext_lb = bw.ext_lb;
     pa.ext_stride = ext_stride;
-    pa.order = reorder ? bw.order : nullptr;
     pa.q_k = rq.q_k;
     pa.q_qprobes = rq.q_qprobes;
     pa.k_uniform = rq.k_uniform;

@@ -9,13 +9,12 @@
 namespace fpp {
 
 // ---------------------------------------------------------------- probe cut
-// k_probe_cut — one block per processing slot (the slot's query is
-// order[slot], or the slot itself): the global top-qProbes of the query's
+// k_probe_cut — one block per query: the global top-qProbes of the query's
 // L * m per-table lists (FalconnPP.cpp:540-582), ranked by counting exactly
 // as the fused kernel's small-list cut does, with the reference's heap
 // replayed when a tie straddles the cut; then the probed buckets' offsets and
 // the inclusive prefix of their sizes.  The fused kernel starts its gather
-// from these, and reads the next slot's ranges to prefetch them.
+// from these.
 constexpr int kPcThreads = 128;
 
 __global__ void __launch_bounds__(kPcThreads) k_probe_cut(ProbeCutArgs a) {
@@ -27,12 +26,11 @@ __global__ void __launch_bounds__(kPcThreads) k_probe_cut(ProbeCutArgs a) {
   __shared__ int hi[2 * kBMaxList];
   __shared__ long long tmp[32];
   const int tid = threadIdx.x;
-  const int slot = blockIdx.x;
-  const int q = a.order ? (int)a.order[slot] : slot;
+  const int q = blockIdx.x;
   const int k = a.q_k ? a.q_k[q] : a.k_uniform;
   const int Qp = a.q_qprobes ? a.q_qprobes[q] : a.qprobes_uniform;
   if (k < 1 || k > a.k_max || Qp < 1 || Qp > a.qprobes_max) {  // the fused kernel rejects the query
-    if (tid == 0) a.pc_n[slot] = 0;
+    if (tid == 0) a.pc_n[q] = 0;
     return;
   }
   const int L = a.L;
@@ -90,7 +88,7 @@ __global__ void __launch_bounds__(kPcThreads) k_probe_cut(ProbeCutArgs a) {
     }
   }
   __syncthreads();
-  const size_t ob = (size_t)slot * a.stride;
+  const size_t ob = (size_t)q * a.stride;
   run = 0;
   for (int base = 0; base < Qp; base += kPcThreads) {
     const int p = base + tid;
@@ -109,7 +107,7 @@ __global__ void __launch_bounds__(kPcThreads) k_probe_cut(ProbeCutArgs a) {
     }
     run += tot;
   }
-  if (tid == 0) a.pc_n[slot] = Qp;
+  if (tid == 0) a.pc_n[q] = Qp;
 }
 
 cudaError_t probe_cut_lists(const ProbeCutArgs& a, int nq, cudaStream_t s) {

@@ -87,9 +87,9 @@ struct BatchArgs {
   const float* ext_lv;
   const uint32_t* ext_lb;
   long long ext_stride;
-  // kHashExt with small lists: k_probe_cut's output per processing slot
-  // (slot * qprobes_max + p): probed global bucket id, bucket offset,
-  // inclusive prefix of the bucket sizes; pc_n[slot] = the slot's qProbes
+  // kHashExt with small lists: k_probe_cut's output per query
+  // (q * qprobes_max + p): probed global bucket id, bucket offset,
+  // inclusive prefix of the bucket sizes; pc_n[q] = the query's qProbes
   const uint32_t* pc_g;
   const uint32_t* pc_o;
   const uint32_t* pc_pe;
@@ -97,12 +97,11 @@ struct BatchArgs {
 };
 
 // Arguments of k_probe_cut (fpp_batch_ext.cu): the probe cut of the split
-// hash's per-table lists, written per processing slot.
+// hash's per-table lists, written per query.
 struct ProbeCutArgs {
   const float* ext_lv;
   const uint32_t* ext_lb;
   long long ext_stride;
-  const uint32_t* order;
   const int* q_k;
   const int* q_qprobes;
   int k_uniform, qprobes_uniform, k_max, qprobes_max;
@@ -296,6 +295,175 @@ __device__ __forceinline__ uint32_t ht_slot(uint32_t id) { return (id * 26544357
 // that share a first slot take different paths (linear probing's clusters
 // made a 256-id step wait for chains of ~11 probes at 55 % fill)
 __device__ __forceinline__ uint32_t ht_step(uint32_t id) { return ((id * 0x85EBCA6Bu) >> (32 - 13)) | 1u; }
+
+// The shortlist, the exact FP32 re-score and the top-k of one query
+// (FalconnPP.cpp:642-706) from its U unique candidates uq[0..U) with their
+// first-pass scores sc[0..U) (FP32 key bits) and the 2048-bin histogram of
+// the scores' top 11 key bits in sm.hist(); the query's FP32 vector is in
+// sm.q.  Writes orow / ovrow.  Every thread of the block calls it.  Returns
+// whether bitset words still need clearing (use_bitset and the unique list
+// kept).
+struct FinishShared {
+  uint32_t* hist;  // 256 bins for the radix selection
+  uint32_t *s_pre, *s_rem;
+  unsigned *s_cnt, *s_sel, *s_bstar, *s_above, *s_inbin;
+  long long* tmp;
+};
+
+template <int MODE, int VI32, int GROUPS>
+__device__ __forceinline__ bool finish_query(const BatchArgs& a, const BatchSmem<GROUPS>& sm,
+                                             unsigned long long* s_top, uint32_t* uq, uint32_t* sc, unsigned U, int k,
+                                             int32_t* orow, float* ovrow, bool use_bitset, uint32_t* bits,
+                                             const FinishShared& fs, int tid, int warp, int lane) {
+  uint32_t* s_hist = sm.hist();
+  const unsigned kk = (unsigned)k;
+  const unsigned R = MODE == kRowsF32 ? kk : min((unsigned)kBMaxTop, kk * (unsigned)a.shortlist_mult);
+  unsigned nsel = U;
+  bool exact = true;
+  uint32_t* sid = sm.sid();
+  uint32_t* ssc = sm.ssc();
+  // the shortlist (ids and first scores) goes to sid/ssc: every candidate
+  // whose key reaches the cut t, which is the bin of the R-th largest key
+  // (refined by the next 11 key bits when that bin holds many)
+  if (U > R) {
+    hist_find(s_hist, R, fs.tmp, fs.s_bstar, fs.s_above, fs.s_inbin);
+    const uint32_t bstar = *fs.s_bstar;
+    const unsigned above = *fs.s_above, inbin = *fs.s_inbin;
+    bool take = true;
+    uint32_t t = bstar << 21;
+    if (above <= (unsigned)kBMaxTop) {
+      if (above > R + R / 2 + 32) {
+        for (int i = tid; i < kHistBins; i += kBThreads) s_hist[i] = 0u;
+        __syncthreads();
+        for (unsigned i = tid; i < U; i += kBThreads) {
+          const uint32_t key = ord_key_bits(sc[i]);
+          if ((key >> 21) == bstar) atomicAdd(s_hist + ((key >> 10) & (kHistBins - 1)), 1u);
+        }
+        __syncthreads();
+        hist_find(s_hist, R - (above - inbin), fs.tmp, fs.s_bstar, fs.s_above, fs.s_inbin);
+        t |= *fs.s_bstar << 10;
+      }
+    } else {
+      // very many equal top bits: radix selection of the R-th key
+      unsigned ge;
+      t = block_select((int)U, R, [&](int i) { return ord_key_bits(sc[i]); }, fs.hist, fs.s_pre, fs.s_rem, fs.s_cnt,
+                       &ge);
+      if (MODE == kRowsF32 && ge != R) {
+        exact = false;
+        take = false;
+      }
+    }
+    if (take) {
+      if (tid == 0) *fs.s_sel = 0;
+      __syncthreads();
+      for (unsigned i = tid; i < U; i += kBThreads) {
+        const uint32_t key = ord_key_bits(sc[i]);
+        if (key >= t) {
+          const unsigned pos = atomicAdd(fs.s_sel, 1u);
+          if (pos < (unsigned)kBMaxTop) {
+            sid[pos] = uq[i];
+            ssc[pos] = sc[i];
+          }
+        }
+      }
+      __syncthreads();
+      nsel = min(*fs.s_sel, (unsigned)kBMaxTop);
+    }
+  } else {
+    for (unsigned i = tid; i < U; i += kBThreads) {
+      sid[i] = uq[i];
+      ssc[i] = sc[i];
+    }
+    __syncthreads();
+  }
+  if (exact) {
+    if (MODE != kRowsF32) {
+      // exact FP32 re-score of the shortlist with the parity dot order
+      rerank_rows<kRowsF32, VI32>(sid, nsel, ssc, sm.q, reinterpret_cast<const unsigned char*>(a.Xc),
+                                  (size_t)a.ld * 4, a.ld / 4, nullptr, warp, kBWarps, lane, nullptr);
+      __syncthreads();
+    }
+    const unsigned kept = min(nsel, kk);
+    unsigned dup = 0;
+    // s_top[0..kept): the best candidates by (score desc, id asc).  Equal
+    // FP32 scores in the kept list, or at the k-th place, leave the order to
+    // the reference's heap (dup).
+    if (nsel <= 2u * kBThreads) {
+      // rank by counting: no sort, two barriers
+      for (unsigned i = tid; i < nsel; i += kBThreads) {
+        const uint32_t ki = ord_key_bits(ssc[i]);
+        const uint32_t ii = sid[i];
+        unsigned gt = 0, eq = 0, before = 0;
+        for (unsigned j = 0; j < nsel; ++j) {
+          const uint32_t kj = ord_key_bits(ssc[j]);
+          gt += kj > ki;
+          eq += kj == ki;
+          before += (kj == ki) & (sid[j] < ii);
+        }
+        const unsigned r = gt + before;
+        if (r < kept) s_top[r] = ((unsigned long long)(~ki) << 32) | ii;
+        dup |= (eq > 1u) & (gt < kk);
+      }
+    } else {
+      for (unsigned i = tid; i < nsel; i += kBThreads)
+        s_top[i] = ((unsigned long long)(~ord_key_bits(ssc[i])) << 32) | sid[i];
+      __syncthreads();
+      block_sort_u64(s_top, (int)nsel);
+      for (unsigned i = tid; i + 1 < nsel && i < kk; i += kBThreads)
+        dup |= (s_top[i] >> 32) == (s_top[i + 1] >> 32);
+    }
+    exact = !__syncthreads_or(dup);
+    if (exact) {
+      for (int j = tid; j < k; j += kBThreads) {
+        if ((unsigned)j < kept) {
+          orow[j] = (int32_t)(uint32_t)s_top[j];
+          if (ovrow) ovrow[j] = __uint_as_float(ord_key_inv_dev(~(uint32_t)(s_top[j] >> 32)));
+        } else {
+          orow[j] = 0;
+          if (ovrow) ovrow[j] = 0.0f;
+        }
+      }
+    }
+  }
+  bool bits_dirty = use_bitset;
+  if (!exact) {
+    // the reference's min-heap over the candidates in ascending id order
+    // (FalconnPP.cpp:633-673): all of them in FP32 mode, the shortlist otherwise
+    const bool whole = (MODE == kRowsF32);
+    const unsigned nc = whole ? U : nsel;
+    uint32_t* cid = uq;
+    uint32_t* csc = sc;
+    if (!whole) {
+      for (unsigned i = tid; i < nc; i += kBThreads) {  // the shortlist with its exact FP32 scores
+        cid[i] = sid[i];
+        csc[i] = ssc[i];
+      }
+      __syncthreads();
+      if (use_bitset) {  // the unique list was overwritten: clear every word
+        for (long long w = tid; w < a.nwords; w += kBThreads) bits[w] = 0u;
+        bits_dirty = false;
+      }
+    }
+    block_bitonic_sort_u32(cid, csc, (int)nc);
+    if (tid == 0) {
+      float* hv = sm.fhv();
+      int* hi = sm.fhi();
+      int n = 0;
+      for (unsigned i = 0; i < nc; ++i) topp_offer<int>(hv, hi, n, k, __uint_as_float(csc[i]), (int)cid[i]);
+      for (int j = n; j < k; ++j) {
+        orow[j] = 0;
+        if (ovrow) ovrow[j] = 0.0f;
+      }
+      for (int j = n - 1; j >= 0; --j) {
+        orow[j] = hi[0];
+        if (ovrow) ovrow[j] = hv[0];
+        heap_pop<true, int>(hv, hi, n);
+      }
+    }
+    __syncthreads();
+  }
+  return bits_dirty;
+}
 
 // HASH: kHashAuto rotates on the tensor cores where a query keeps one probe
 // per table (and a.tflips is set), exactly otherwise; kHashTC only on the
@@ -585,7 +753,7 @@ __global__ void __launch_bounds__(kBThreads, MODE == kRowsF32 ? 2 : 3) k_batch_q
     uint32_t* s_pe = BIGL ? a.gpe + (size_t)blockIdx.x * a.probe_cap : sm.pe();
     if constexpr (PCUT) {
       // the ranges of the slot's probes, and their ids on the way to L2
-      const size_t pb = (size_t)qu * a.qprobes_max;
+      const size_t pb = (size_t)q * a.qprobes_max;
       for (int p = tid; p < Qp; p += kBThreads) {
         const uint32_t pe = a.pc_pe[pb + p];
         const uint32_t ex = p ? a.pc_pe[pb + p - 1] : 0u;
@@ -799,151 +967,9 @@ __global__ void __launch_bounds__(kBThreads, MODE == kRowsF32 ? 2 : 3) k_batch_q
     __syncthreads();
 
     // ---- 5. shortlist by the first scores, exact FP32 re-score, top-k
-    const unsigned kk = (unsigned)k;
-    const unsigned R = MODE == kRowsF32 ? kk : min((unsigned)kBMaxTop, kk * (unsigned)a.shortlist_mult);
-    unsigned nsel = U;
-    bool exact = true;
-    uint32_t* sid = sm.sid();
-    uint32_t* ssc = sm.ssc();
-    // the shortlist (ids and first scores) goes to sid/ssc: every candidate
-    // whose key reaches the cut t, which is the bin of the R-th largest key
-    // (refined by the next 11 key bits when that bin holds many)
-    if (U > R) {
-      hist_find(s_hist, R, tmp, &s_bstar, &s_above, &s_inbin);
-      const uint32_t bstar = s_bstar;
-      const unsigned above = s_above, inbin = s_inbin;
-      bool take = true;
-      uint32_t t = bstar << 21;
-      if (above <= (unsigned)kBMaxTop) {
-        if (above > R + R / 2 + 32) {
-          for (int i = tid; i < kHistBins; i += kBThreads) s_hist[i] = 0u;
-          __syncthreads();
-          for (unsigned i = tid; i < U; i += kBThreads) {
-            const uint32_t key = ord_key_bits(sc[i]);
-            if ((key >> 21) == bstar) atomicAdd(s_hist + ((key >> 10) & (kHistBins - 1)), 1u);
-          }
-          __syncthreads();
-          hist_find(s_hist, R - (above - inbin), tmp, &s_bstar, &s_above, &s_inbin);
-          t |= s_bstar << 10;
-        }
-      } else {
-        // very many equal top bits: radix selection of the R-th key
-        unsigned ge;
-        t = block_select((int)U, R, [&](int i) { return ord_key_bits(sc[i]); }, hist, &s_pre, &s_rem, &s_cnt, &ge);
-        if (MODE == kRowsF32 && ge != R) {
-          exact = false;
-          take = false;
-        }
-      }
-      if (take) {
-        if (tid == 0) s_sel = 0;
-        __syncthreads();
-        for (unsigned i = tid; i < U; i += kBThreads) {
-          const uint32_t key = ord_key_bits(sc[i]);
-          if (key >= t) {
-            const unsigned pos = atomicAdd(&s_sel, 1u);
-            if (pos < (unsigned)kBMaxTop) {
-              sid[pos] = uq[i];
-              ssc[pos] = sc[i];
-            }
-          }
-        }
-        __syncthreads();
-        nsel = min(s_sel, (unsigned)kBMaxTop);
-      }
-    } else {
-      for (unsigned i = tid; i < U; i += kBThreads) {
-        sid[i] = uq[i];
-        ssc[i] = sc[i];
-      }
-      __syncthreads();
-    }
-    if (exact) {
-      if (MODE != kRowsF32) {
-        // exact FP32 re-score of the shortlist with the parity dot order
-        rerank_rows<kRowsF32, VI32>(sid, nsel, ssc, sm.q, reinterpret_cast<const unsigned char*>(a.Xc),
-                                    (size_t)a.ld * 4, a.ld / 4, nullptr, warp, kBWarps, lane, nullptr);
-        __syncthreads();
-      }
-      const unsigned kept = min(nsel, kk);
-      unsigned dup = 0;
-      // s_top[0..kept): the best candidates by (score desc, id asc).  Equal
-      // FP32 scores in the kept list, or at the k-th place, leave the order to
-      // the reference's heap (dup).
-      if (nsel <= 2u * kBThreads) {
-        // rank by counting: no sort, two barriers
-        for (unsigned i = tid; i < nsel; i += kBThreads) {
-          const uint32_t ki = ord_key_bits(ssc[i]);
-          const uint32_t ii = sid[i];
-          unsigned gt = 0, eq = 0, before = 0;
-          for (unsigned j = 0; j < nsel; ++j) {
-            const uint32_t kj = ord_key_bits(ssc[j]);
-            gt += kj > ki;
-            eq += kj == ki;
-            before += (kj == ki) & (sid[j] < ii);
-          }
-          const unsigned r = gt + before;
-          if (r < kept) s_top[r] = ((unsigned long long)(~ki) << 32) | ii;
-          dup |= (eq > 1u) & (gt < kk);
-        }
-      } else {
-        for (unsigned i = tid; i < nsel; i += kBThreads)
-          s_top[i] = ((unsigned long long)(~ord_key_bits(ssc[i])) << 32) | sid[i];
-        __syncthreads();
-        block_sort_u64(s_top, (int)nsel);
-        for (unsigned i = tid; i + 1 < nsel && i < kk; i += kBThreads)
-          dup |= (s_top[i] >> 32) == (s_top[i + 1] >> 32);
-      }
-      exact = !__syncthreads_or(dup);
-      if (exact) {
-        for (int j = tid; j < k; j += kBThreads) {
-          if ((unsigned)j < kept) {
-            orow[j] = (int32_t)(uint32_t)s_top[j];
-            if (ovrow) ovrow[j] = __uint_as_float(ord_key_inv_dev(~(uint32_t)(s_top[j] >> 32)));
-          } else {
-            orow[j] = 0;
-            if (ovrow) ovrow[j] = 0.0f;
-          }
-        }
-      }
-    }
-    bool bits_dirty = use_bitset;
-    if (!exact) {
-      // the reference's min-heap over the candidates in ascending id order
-      // (FalconnPP.cpp:633-673): all of them in FP32 mode, the shortlist otherwise
-      const bool whole = (MODE == kRowsF32);
-      const unsigned nc = whole ? U : nsel;
-      uint32_t* cid = uq;
-      uint32_t* csc = sc;
-      if (!whole) {
-        for (unsigned i = tid; i < nc; i += kBThreads) {  // the shortlist with its exact FP32 scores
-          cid[i] = sid[i];
-          csc[i] = ssc[i];
-        }
-        __syncthreads();
-        if (use_bitset) {  // the unique list was overwritten: clear every word
-          for (long long w = tid; w < a.nwords; w += kBThreads) bits[w] = 0u;
-          bits_dirty = false;
-        }
-      }
-      block_bitonic_sort_u32(cid, csc, (int)nc);
-      if (tid == 0) {
-        float* hv = sm.fhv();
-        int* hi = sm.fhi();
-        int n = 0;
-        for (unsigned i = 0; i < nc; ++i) topp_offer<int>(hv, hi, n, k, __uint_as_float(csc[i]), (int)cid[i]);
-        for (int j = n; j < k; ++j) {
-          orow[j] = 0;
-          if (ovrow) ovrow[j] = 0.0f;
-        }
-        for (int j = n - 1; j >= 0; --j) {
-          orow[j] = hi[0];
-          if (ovrow) ovrow[j] = hv[0];
-          heap_pop<true, int>(hv, hi, n);
-        }
-      }
-      __syncthreads();
-    }
+    const FinishShared fs{hist, &s_pre, &s_rem, &s_cnt, &s_sel, &s_bstar, &s_above, &s_inbin, tmp};
+    const bool bits_dirty =
+        finish_query<MODE, VI32, GROUPS>(a, sm, s_top, uq, sc, U, k, orow, ovrow, use_bitset, bits, fs, tid, warp, lane);
     // ---- 6. leave the hash set empty and the bitset clear
     {
       const uint4 e4 = make_uint4(kEmpty, kEmpty, kEmpty, kEmpty);
