@@ -704,7 +704,12 @@ extern "C" int fpp_bruteforce_topk_lowp(fpp_index* h, const float* d_queries, in
   // P units per CTA, then the unit length that spreads the tiles over nsm x P
   // units: every SM gets the same work
   const long long per_cta = std::max<long long>(1, (T + (long long)nsm * tu_max - 1) / ((long long)nsm * tu_max));
-  const long long tu = std::max<long long>(1, (T + (long long)nsm * per_cta - 1) / ((long long)nsm * per_cta));
+  // few query tiles: units long enough that a query tile's segments fit the
+  // merge (at most kMergeMax / RS, one more where a unit straddles two tiles)
+  const long long seg_max = kMergeMax / RS - 1;
+  const long long tu_merge = (xtiles + seg_max - 1) / seg_max;
+  const long long tu = std::max<long long>(
+      {1LL, tu_merge, (T + (long long)nsm * per_cta - 1) / ((long long)nsm * per_cta)});
   const long long units = (T + tu - 1) / tu;
   const long long grid = (units + per_cta - 1) / per_cta;
   const long long max_segs = (xtiles + tu - 1) / tu + 1;

@@ -115,6 +115,20 @@ def test_crowded_neighbours(precision):
     g.close()
 
 
+@pytest.mark.parametrize("nq", [1, 5, 129])
+def test_few_queries_many_rows(nq):
+    # one query tile against 1,563 row tiles: the units grow so that the
+    # tile's segments fit the merge
+    X = synth.mixture(200_000, 64, n_centres=32, seed=0)
+    Q = synth.mixture(nq, 64, n_centres=32, seed=1)
+    g = _index(X)
+    ids, val = _lowp(g, Q, 10, 1, 4)
+    ref, _ = _fp64(X, Q, 10)
+    assert synth.recall_at_k(ref, ids, 10) >= 0.99
+    assert np.all(np.diff(val, axis=1) <= 0)
+    g.close()
+
+
 def test_rejections():
     X = synth.mixture(2000, 64, n_centres=4, seed=0)
     g = _index(X)
