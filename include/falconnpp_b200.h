@@ -109,7 +109,11 @@ int fpp_get_stats(fpp_index* h, int kind, double* out, int n);
  * (batched form: resident blocks per SM, 0 = occupancy limit),
  * "reorder_queries" (default 1: the batched form processes a batch grouped by
  * the first table's first-layer bucket code, so queries in flight together
- * share buckets and rows in L2; results are unchanged), "tc_rotation"
+ * share buckets and rows in L2; results are unchanged), "split_hash" (default
+ * 1: the batched form hashes in its own exact FP32 kernel, then runs the probe
+ * cut of every query in its own kernel, before the fused gather / rerank /
+ * top-k kernel; 0: one fused kernel that also rotates and hashes; the results
+ * are the same), "tc_rotation"
  * (default 0, opt-in: the batched BF16/FP8 form with fhtDim 256 and one probe
  * per table rotates on the tensor cores with FP16 operands and FP32
  * accumulation instead of the reference's FP32 arithmetic; its probes can then
