@@ -183,6 +183,8 @@ void BatchWorkspace::release() {
   cudaFree(counters);
   for (auto& ev : tev)
     if (ev) cudaEventDestroy(ev);
+  for (auto& ev : cev)
+    if (ev) cudaEventDestroy(ev);
   cudaFree(okey);
   cudaFree(ohist);
   cudaFree(order);
@@ -347,10 +349,43 @@ int batch_query(const Params& P, DeviceIndex& di, BatchWorkspace& bw, const Batc
         if (!ev && (e = cudaEventCreate(&ev)) != cudaSuccess) return fail(e, "event create");
       cudaEventRecord(bw.tev[0], s);
     }
-    if ((e = hash_lists(P, di, rq.Q, rq.nq, rq.q_qprobes, rq.qprobes_max, bw.ext_lv, bw.ext_lb, ext_stride,
-                        bw.hheap_v, bw.hheap_i, max_groups, s)) != cudaSuccess)
-      return fail(e, "hash kernel");
+    // host queries: four chunks copied on the copy stream, each hashed as
+    // soon as it lands
+    const int nch = (rq.Q_host && rq.copy_stream && rq.copy_stream != s && rq.nq >= 4096) ? 4 : 1;
+    if (rq.Q_host && nch == 1 &&
+        (e = cudaMemcpyAsync(const_cast<float*>(rq.Q), rq.Q_host, sizeof(float) * (size_t)rq.nq * d,
+                             cudaMemcpyHostToDevice, s)) != cudaSuccess)
+      return fail(e, "query copy");
+    if (nch > 1) {
+      for (auto& ev : bw.cev)
+        if (!ev && (e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess)
+          return fail(e, "event create");
+      // the copies wait for the stream's earlier work (a previous batch may
+      // still read the query buffer)
+      cudaEventRecord(bw.cev[4], s);
+      cudaStreamWaitEvent(rq.copy_stream, bw.cev[4], 0);
+      for (int c = 0; c < nch; ++c) {
+        const long long q0 = (long long)rq.nq * c / nch, q1 = (long long)rq.nq * (c + 1) / nch;
+        if ((e = cudaMemcpyAsync(const_cast<float*>(rq.Q) + q0 * d, rq.Q_host + q0 * d,
+                                 sizeof(float) * (size_t)(q1 - q0) * d, cudaMemcpyHostToDevice, rq.copy_stream)) !=
+            cudaSuccess)
+          return fail(e, "query copy");
+        cudaEventRecord(bw.cev[c], rq.copy_stream);
+      }
+    }
+    for (int c = 0; c < nch; ++c) {
+      const long long q0 = (long long)rq.nq * c / nch, q1 = (long long)rq.nq * (c + 1) / nch;
+      if (nch > 1) cudaStreamWaitEvent(s, bw.cev[c], 0);
+      if ((e = hash_lists(P, di, rq.Q + q0 * d, (int)(q1 - q0), rq.q_qprobes ? rq.q_qprobes + q0 : nullptr,
+                          rq.qprobes_max, bw.ext_lv + q0 * ext_stride, bw.ext_lb + q0 * ext_stride, ext_stride,
+                          bw.hheap_v, bw.hheap_i, max_groups, s)) != cudaSuccess)
+        return fail(e, "hash kernel");
+    }
     if (rq.stage_timing) cudaEventRecord(bw.tev[3], s);
+  } else if (rq.Q_host) {
+    if ((e = cudaMemcpyAsync(const_cast<float*>(rq.Q), rq.Q_host, sizeof(float) * (size_t)rq.nq * d,
+                             cudaMemcpyHostToDevice, s)) != cudaSuccess)
+      return fail(e, "query copy");
   }
   // query order (worth it once the batch is a few waves of blocks)
   int log2D = 0;

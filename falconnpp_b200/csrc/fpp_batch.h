@@ -26,6 +26,11 @@ struct BatchRequest {
   uint32_t* dump_probes = nullptr;  // parity dumps (device, nullable; no graph): [nq][qprobes_max] probes
   uint32_t* dump_counts = nullptr;  // [nq][2] candidates, unique candidates
   bool split_hash = true;           // exact hash in its own kernel before the fused one (kHashExt)
+  // host queries (nullable): batch_query copies them into Q (device, nq x d)
+  // itself; with the split hash, in chunks on copy_stream, each chunk's hash
+  // launch waiting only for its own chunk, so the copy overlaps the hashing
+  const float* Q_host = nullptr;
+  cudaStream_t copy_stream = nullptr;
   bool stage_timing = false;        // CUDA events around the hash and the fused kernel (synchronises)
   bool tc_rotation = false;        // opt-in, BF16/FP8, fhtDim 256: rotate on the tensor cores (FP16 operands,
                                    // not the reference's FP32 hash: probes can differ)
@@ -110,6 +115,7 @@ struct BatchWorkspace {
   int* pc_n = nullptr;
   long long pc_cap = 0, pc_ncap = 0;
   cudaEvent_t tev[4] = {nullptr, nullptr, nullptr, nullptr};  // stage timing: start, fused start, end, hash end
+  cudaEvent_t cev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};  // chunked query copy: chunks, start
   cudaGraphExec_t graph_exec = nullptr;
   cudaGraph_t graph = nullptr;
   cudaGraphNode_t graph_knode = nullptr;

@@ -148,9 +148,11 @@ void print_build(const fpp_index* h) {
 // the caller reads the status words (h->bw.counters + 1) after its own copies
 // and reports an overflow with batched_overflow_error().
 int run_batched(fpp_index* h, const float* dQ, int nq, int k, int32_t* dout, cudaStream_t s,
-                bool check_status = true) {
+                bool check_status = true, const float* Q_host = nullptr, cudaStream_t copy_stream = nullptr) {
   fpp::BatchRequest rq;
   rq.Q = dQ;
+  rq.Q_host = Q_host;
+  rq.copy_stream = copy_stream;
   rq.nq = nq;
   rq.k_uniform = k;
   rq.qprobes_uniform = h->P.qProbes;
@@ -240,6 +242,7 @@ void fpp_destroy(fpp_index* h) {
     h->bfw.release();
     fpp::free_index(h->di);
     if (h->stream) cudaStreamDestroy(h->stream);
+    if (h->cstream) cudaStreamDestroy(h->cstream);
   }
   delete h;
 }
@@ -385,9 +388,12 @@ int fpp_query(fpp_index* h, const float* queries, int n_queries, int n_neighbors
       if (e == cudaSuccess) h->ws.cap_out = (size_t)n_queries * n_neighbors;
     }
     if (e != cudaSuccess) return fail(FPP_ERR_OUT_OF_MEMORY, std::string("query: ") + cudaGetErrorString(e));
-    cudaMemcpyAsync(h->ws.Qd, queries, sizeof(float) * n_queries * P.n_features, cudaMemcpyHostToDevice, h->stream);
-    // one synchronisation: results and the kernel's status words come back together
-    rc = run_batched(h, h->ws.Qd, n_queries, n_neighbors, h->ws.out, h->stream, false);
+    if (!h->cstream && cudaStreamCreateWithFlags(&h->cstream, cudaStreamNonBlocking) != cudaSuccess)
+      h->cstream = nullptr;
+    // the queries are copied by the batched form itself (in chunks that
+    // overlap the hashing); one synchronisation: results and the kernel's
+    // status words come back together
+    rc = run_batched(h, h->ws.Qd, n_queries, n_neighbors, h->ws.out, h->stream, false, queries, h->cstream);
     if (rc) return rc;
     unsigned status = 0;
     e = cudaMemcpyAsync(out, h->ws.out, sizeof(int32_t) * n_queries * n_neighbors, cudaMemcpyDeviceToHost, h->stream);

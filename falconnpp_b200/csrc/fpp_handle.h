@@ -31,6 +31,7 @@ struct fpp_index {
   bool built = false;
   int device = 0;
   cudaStream_t stream = nullptr;
+  cudaStream_t cstream = nullptr;  // host-buffer batched queries: the chunked query copies
   std::mutex mu;
 };
 

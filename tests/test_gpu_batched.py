@@ -178,3 +178,25 @@ def test_hash_set_overflow_falls_back_to_bitset(precision):
     else:
         assert synth.recall_at_k(plain, got, 10) >= 0.9
     assert np.array_equal(_batched(g, Q, 10, 32, precision=precision, mult=4), got)
+
+
+@pytest.mark.parametrize("precision", [0, 1, 2])
+def test_host_queries_equal_device_queries(precision):
+    # fpp_query with host buffers copies large batches in chunks that overlap
+    # the hash kernel; the results must be the device-pointer path's
+    import torch
+    X = synth.mixture(50_000, 200, n_centres=32, seed=0)
+    Q = synth.mixture(6001, 200, n_centres=32, seed=1)
+    g = _index(X, 16, 256, 100, 0.01, 3)
+    g.set_qprobes(6)
+    g.set_query_form(1, precision, 2)
+    for graph in (0, 1):
+        g.set_option("use_graph", graph)
+        host = g.query(Q, 10)
+        dq = torch.from_numpy(Q).cuda()
+        out = torch.zeros((len(Q), 10), dtype=torch.int32, device="cuda")
+        g.query_device(dq.data_ptr(), len(Q), 10, out.data_ptr())
+        torch.cuda.synchronize()
+        assert np.array_equal(host, out.cpu().numpy())
+        assert np.array_equal(host, g.query(Q, 10))  # the query buffer is reused safely
+    g.close()
