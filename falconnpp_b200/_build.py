@@ -22,7 +22,8 @@ CSRC = os.path.join(HERE, "csrc")
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libfalconnpp_b200.so")
 CU_SOURCES = ["fpp_build.cu", "fpp_query.cu", "fpp_capi.cu", "fpp_batch.cu", "fpp_batch_f32.cu", "fpp_batch_bf16.cu",
-              "fpp_batch_fp8.cu", "fpp_batch_big.cu", "fpp_batch_ext.cu", "fpp_noalloc.cu", "fpp_server.cu", "fpp_bruteforce.cu", "fpp_bf_lowp.cu", "fpp_persist.cu"]
+              "fpp_batch_fp8.cu", "fpp_batch_big.cu", "fpp_batch_ext.cu", "fpp_noalloc.cu", "fpp_server.cu", "fpp_bruteforce.cu", "fpp_bf_lowp.cu", "fpp_persist.cu",
+              "fpp_hash_verify.cu"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17", "-fmad=false", "-ftz=false", "-prec-div=true", "-prec-sqrt=true",

@@ -204,8 +204,8 @@ class Index:
                     device=int(v[5]), n_tables=int(v[6]), n_proj=int(v[7]), iProbes=int(v[8]))
 
     def stats(self, kind: int) -> np.ndarray:
-        v = np.zeros(10, np.float64)
-        _check(lib().fpp_get_stats(self.h, kind, _ptr(v), 10))
+        v = np.zeros(11, np.float64)
+        _check(lib().fpp_get_stats(self.h, kind, _ptr(v), 11))
         return v
 
     def dump_bits(self):

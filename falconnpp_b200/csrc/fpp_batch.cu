@@ -318,6 +318,7 @@ int batch_query(const Params& P, DeviceIndex& di, BatchWorkspace& bw, const Batc
   }
   grid = std::min(grid, bw.grid);
   const long long ext_stride = (long long)L * std::max(mmax, 1);
+  const bool vhash = split && rq.tc_hash && F == 256 && di.tflips && L <= 128 && 2 * rq.qprobes_max <= L;
   if (split) {
     const long long max_groups = (long long)nsm * 64;
     if (!bw.ext_lv || bw.ext_cap < (long long)rq.nq * ext_stride) {
@@ -347,6 +348,8 @@ int batch_query(const Params& P, DeviceIndex& di, BatchWorkspace& bw, const Batc
     if (rq.stage_timing) {
       for (auto& ev : bw.tev)
         if (!ev && (e = cudaEventCreate(&ev)) != cudaSuccess) return fail(e, "event create");
+      if (vhash && (e = cudaMemsetAsync(bw.counters + 2, 0, sizeof(unsigned), s)) != cudaSuccess)
+        return fail(e, "memset");
       cudaEventRecord(bw.tev[0], s);
     }
     // host queries: four chunks copied on the copy stream, each hashed as
@@ -376,10 +379,13 @@ int batch_query(const Params& P, DeviceIndex& di, BatchWorkspace& bw, const Batc
     for (int c = 0; c < nch; ++c) {
       const long long q0 = (long long)rq.nq * c / nch, q1 = (long long)rq.nq * (c + 1) / nch;
       if (nch > 1) cudaStreamWaitEvent(s, bw.cev[c], 0);
-      if ((e = hash_lists(P, di, rq.Q + q0 * d, (int)(q1 - q0), rq.q_qprobes ? rq.q_qprobes + q0 : nullptr,
-                          rq.qprobes_max, bw.ext_lv + q0 * ext_stride, bw.ext_lb + q0 * ext_stride, ext_stride,
-                          bw.hheap_v, bw.hheap_i, max_groups, s)) != cudaSuccess)
-        return fail(e, "hash kernel");
+      const int* qq = rq.q_qprobes ? rq.q_qprobes + q0 : nullptr;
+      e = vhash ? hash_lists_verified(P, di, rq.Q + q0 * d, (int)(q1 - q0), qq, rq.qprobes_max,
+                                      bw.ext_lv + q0 * ext_stride, bw.ext_lb + q0 * ext_stride, ext_stride,
+                                      rq.stage_timing ? bw.counters + 2 : nullptr, s)
+                : hash_lists(P, di, rq.Q + q0 * d, (int)(q1 - q0), qq, rq.qprobes_max, bw.ext_lv + q0 * ext_stride,
+                             bw.ext_lb + q0 * ext_stride, ext_stride, bw.hheap_v, bw.hheap_i, max_groups, s);
+      if (e != cudaSuccess) return fail(e, "hash kernel");
     }
     if (rq.stage_timing) cudaEventRecord(bw.tev[3], s);
   } else if (rq.Q_host) {
@@ -608,6 +614,12 @@ int batch_query(const Params& P, DeviceIndex& di, BatchWorkspace& bw, const Batc
     cudaEventElapsedTime(&res.ms_hash, bw.tev[0], bw.tev[3]);
     cudaEventElapsedTime(&res.ms_prep, bw.tev[3], bw.tev[1]);
     cudaEventElapsedTime(&res.ms_fused, bw.tev[1], bw.tev[2]);
+    if (vhash) {
+      unsigned nx = 0;
+      if ((e = cudaMemcpy(&nx, bw.counters + 2, sizeof(unsigned), cudaMemcpyDeviceToHost)) != cudaSuccess)
+        return fail(e, "stage timing");
+      res.tc_exact = nx;
+    }
   }
   res.grid = grid;
   if (rq.check_status) {

@@ -26,6 +26,10 @@ struct BatchRequest {
   uint32_t* dump_probes = nullptr;  // parity dumps (device, nullable; no graph): [nq][qprobes_max] probes
   uint32_t* dump_counts = nullptr;  // [nq][2] candidates, unique candidates
   bool split_hash = true;           // exact hash in its own kernel before the fused one (kHashExt)
+  // split hash, fhtDim 256, L <= 128, 2 qProbes <= L: rotate on the tensor
+  // cores and hash again in FP32 every table that can reach the probe cut
+  // (k_query_hash_verified); the probes and their scores are unchanged
+  bool tc_hash = true;
   // host queries (nullable): batch_query copies them into Q (device, nq x d)
   // itself; with the split hash, in chunks on copy_stream, each chunk's hash
   // launch waiting only for its own chunk, so the copy overlaps the hashing
@@ -45,6 +49,7 @@ struct BatchResult {
   // with stage_timing: the hash kernel (split form), the order and probe-cut
   // kernels, and the fused kernel
   float ms_hash = 0, ms_prep = 0, ms_fused = 0;
+  long long tc_exact = 0;           // with stage_timing: tables the verified hash re-hashed in FP32
 };
 
 struct BatchKey {

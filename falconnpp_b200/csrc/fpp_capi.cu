@@ -143,6 +143,19 @@ void print_build(const fpp_index* h) {
             << " seconds" << std::endl;
 }
 
+// The query statistics of a batched call: kernels launched and, with
+// "stage_timing", the CUDA-event milliseconds of the hash kernel (split form),
+// the order and probe-cut kernels and the fused gather / rerank / top-k
+// kernel, and the tables the verified tensor-core hash re-hashed in FP32.
+void set_batch_stats(fpp_index* h, const fpp::BatchResult& res) {
+  h->qst = fpp::QueryStats();
+  h->qst.launches = res.launches;
+  h->qst.ms_hash = res.ms_hash;
+  h->qst.ms_select = res.ms_prep;
+  h->qst.ms_rerank = res.ms_fused;
+  h->qst.tc_exact = res.tc_exact;
+}
+
 // Runs the batched form for device queries/outputs (uniform k, the handle's
 // qProbes).  With check_status false the call does not wait for the kernel;
 // the caller reads the status words (h->bw.counters + 1) after its own copies
@@ -167,6 +180,7 @@ int run_batched(fpp_index* h, const float* dQ, int nq, int k, int32_t* dout, cud
   rq.reorder = h->reorder;
   rq.tc_rotation = h->tc_rotation;
   rq.split_hash = h->split_hash;
+  rq.tc_hash = h->tc_hash;
   rq.stage_timing = h->ws.stage_timing;
   rq.check_status = check_status;
   fpp::BatchResult res;
@@ -174,12 +188,8 @@ int run_batched(fpp_index* h, const float* dQ, int nq, int k, int32_t* dout, cud
   const int rc = fpp::batch_query(h->P, h->di, h->bw, rq, s, res, err);
   if (rc) return fail(rc, err.msg);
   if (res.overflow) return fail(FPP_ERR_UNSUPPORTED, "batched query: candidate capacity exceeded");
-  h->qst = fpp::QueryStats();
-  h->qst.launches = res.launches;
+  set_batch_stats(h, res);
   h->qst.total_probes = (long long)nq * h->P.qProbes;
-  h->qst.ms_hash = res.ms_hash;     // with "stage_timing": the exact hash kernel (split form),
-  h->qst.ms_select = res.ms_prep;   // the order and probe-cut kernels,
-  h->qst.ms_rerank = res.ms_fused;  // and the fused gather / rerank / top-k kernel
   return FPP_OK;
 }
 
@@ -317,6 +327,8 @@ int fpp_set_option(fpp_index* h, const char* key, long long value) {
     h->tc_rotation = value != 0;
   } else if (!strcmp(key, "split_hash")) {
     h->split_hash = value != 0;
+  } else if (!strcmp(key, "tc_hash")) {
+    h->tc_hash = value != 0;
   } else if (!strcmp(key, "blocks_per_sm")) {
     if (value < 0) return fail(FPP_ERR_INVALID_ARGUMENT, "set_option: blocks_per_sm must be >= 0");
     h->blocks_per_sm = (int)value;
@@ -501,6 +513,7 @@ int fpp_autotune(fpp_index* h, const float* d_queries, int n_queries, int k, dou
     rq.reorder = reorder;
     rq.tc_rotation = h->tc_rotation;
     rq.split_hash = split;
+    rq.tc_hash = h->tc_hash;
     rq.check_status = true;
     fpp::BatchResult res;
     fpp::Error err{0, ""};
@@ -625,6 +638,7 @@ int fpp_query_batched(fpp_index* h, const float* d_queries, int n_queries, const
   rq.reorder = h->reorder;
   rq.tc_rotation = h->tc_rotation;
   rq.split_hash = h->split_hash;
+  rq.tc_hash = h->tc_hash;
   rq.check_status = true;
   fpp::BatchResult res;
   fpp::Error err{0, ""};
@@ -633,8 +647,7 @@ int fpp_query_batched(fpp_index* h, const float* d_queries, int n_queries, const
   if (res.overflow) return fail(FPP_ERR_UNSUPPORTED, "query_batched: candidate capacity exceeded");
   if (res.bad_params)
     return fail(FPP_ERR_INVALID_ARGUMENT, "query_batched: a per-query k or qProbes is outside [1, k_max/qprobes_max]");
-  h->qst = fpp::QueryStats();
-  h->qst.launches = res.launches;
+  set_batch_stats(h, res);
   return ok();
 }
 
@@ -664,14 +677,17 @@ int fpp_query_batched_dump(fpp_index* h, const float* d_queries, int n_queries, 
   rq.reorder = h->reorder;
   rq.tc_rotation = h->tc_rotation;
   rq.split_hash = h->split_hash;
+  rq.tc_hash = h->tc_hash;
   rq.dump_probes = d_probes;
   rq.dump_counts = d_counts;
   rq.check_status = true;
+  rq.stage_timing = h->ws.stage_timing;
   fpp::BatchResult res;
   fpp::Error err{0, ""};
   rc = fpp::batch_query(h->P, h->di, h->bw, rq, s, res, err);
   if (rc) return fail(rc, err.msg);
   if (res.overflow) return fail(FPP_ERR_UNSUPPORTED, "query_batched_dump: candidate capacity exceeded");
+  set_batch_stats(h, res);
   return ok();
 }
 
@@ -740,10 +756,10 @@ int fpp_get_stats(fpp_index* h, int kind, double* out, int n) {
     for (int i = 0; i < n && i < 8; ++i) out[i] = v[i];
   } else if (kind == 1) {
     const fpp::QueryStats& s = h->qst;
-    const double v[10] = {(double)s.total_cand, (double)s.total_unique, (double)s.total_empty,
+    const double v[11] = {(double)s.total_cand, (double)s.total_unique, (double)s.total_empty,
                           (double)s.total_probes, (double)s.n_select_ties, (double)s.n_topk_ties,
-                          (double)s.launches, s.ms_hash, s.ms_select, s.ms_rerank};
-    for (int i = 0; i < n && i < 10; ++i) out[i] = v[i];
+                          (double)s.launches, s.ms_hash, s.ms_select, s.ms_rerank, (double)s.tc_exact};
+    for (int i = 0; i < n && i < 11; ++i) out[i] = v[i];
   } else {
     return fail(FPP_ERR_INVALID_ARGUMENT, "get_stats: kind must be 0 or 1");
   }

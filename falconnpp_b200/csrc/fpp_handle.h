@@ -25,6 +25,7 @@ struct fpp_index {
   bool use_graph = false;   // batched form: capture/replay the launch as a CUDA graph
   int blocks_per_sm = 0;    // batched form: 0 = occupancy limit
   bool reorder = true;      // batched form: process queries grouped by a locality key
+  bool tc_hash = true;      // split hash: tensor-core rotation verified by an exact FP32 re-hash near the cut
   bool split_hash = true;   // batched form: exact hash in its own kernel before the fused one
   bool tc_rotation = false;  // opt-in: batched BF16/FP8 tensor-core rotation (FP16 operands; not bit-exact)
   bool params_set = false;

@@ -59,6 +59,7 @@ struct QueryStats {
   long long launches = 0;      // kernels launched by the call
   // CUDA-event durations on the launching stream (only with stage timing on)
   double ms_hash = 0, ms_select = 0, ms_rerank = 0;
+  long long tc_exact = 0;  // batched form with stage timing: tables re-hashed in FP32 by the verified hash
 };
 
 // Optional host-side dumps for parity checks (any pointer may be null).
@@ -81,6 +82,15 @@ struct QueryDumps {
 cudaError_t hash_lists(const Params& P, const DeviceIndex& di, const float* Q, int nq, const int* q_qprobes, int qp_max,
                        float* list_v, uint32_t* list_b, long long stride, float* heap_v, int* heap_i,
                        long long max_groups, cudaStream_t s);
+
+// The same lists for fhtDim 256 when every query keeps one probe per table
+// (2 qp_max <= L, L <= 128): the rotations on the tensor cores, and an exact
+// FP32 re-hash of every table whose score can reach the probe cut (ties at
+// the cut: of every table), so the probe cut selects the same probes with the
+// same scores.  n_exact (device, nullable) += the tables re-hashed.
+cudaError_t hash_lists_verified(const Params& P, const DeviceIndex& di, const float* Q, int nq, const int* q_qprobes,
+                                int qp_max, float* list_v, uint32_t* list_b, long long stride, unsigned* n_exact,
+                                cudaStream_t s);
 
 int query_index(const Params& P, const DeviceIndex& di, const float* Q, bool q_on_device, int nq, int k,
                 int32_t* out, bool out_on_device, QueryWorkspace& ws, QueryStats& st, cudaStream_t s,

@@ -139,6 +139,7 @@ fpp::BatchRequest slot_request(const fpp_server* S, const Slot& s, int nq) {
   rq.reorder = h->reorder;
   rq.tc_rotation = h->tc_rotation;
   rq.split_hash = h->split_hash;
+  rq.tc_hash = h->tc_hash;
   return rq;
 }
 

@@ -96,8 +96,10 @@ int fpp_get_info(fpp_index* h, long long* out, int n);
  *        probe-cut replays, top-k replays (all summed over the queries),
  *        kernels launched, then (with the "stage_timing" option) the CUDA-event
  *        milliseconds of the hashing, probe-selection and gather/rerank kernels
- *        (batched form: the exact hash kernel, the order and probe-cut
- *        kernels, and the fused kernel). */
+ *        (batched form: the hash kernel, the order and probe-cut kernels, and
+ *        the fused kernel), and (batched form with stage timing) the tables
+ *        the verified tensor-core hash re-hashed in FP32, summed over the
+ *        queries. */
 int fpp_get_stats(fpp_index* h, int kind, double* out, int n);
 
 /* Tuning and test switches: "exact_bucket_order" (default 1: bucket contents
@@ -113,7 +115,14 @@ int fpp_get_stats(fpp_index* h, int kind, double* out, int n);
  * 1: the batched form hashes in its own exact FP32 kernel, then runs the probe
  * cut of every query in its own kernel, before the fused gather / rerank /
  * top-k kernel; 0: one fused kernel that also rotates and hashes; the results
- * are the same), "tc_rotation"
+ * are the same), "tc_hash" (default
+ * 1: with the split hash, fhtDim 256, n_tables <= 128 and 2 qProbes <=
+ * n_tables, the hash kernel rotates on the tensor cores with FP16 operands,
+ * bounds the error of every table's score from the query's norm, and hashes
+ * again in the reference's FP32 arithmetic every table whose score can reach
+ * the probe cut (every table when exact scores tie at the cut); the probes
+ * and their scores are those of the exact hash; 0: the exact FP32 hash of
+ * every table), "tc_rotation"
  * (default 0, opt-in: the batched BF16/FP8 form with fhtDim 256 and one probe
  * per table rotates on the tensor cores with FP16 operands and FP32
  * accumulation instead of the reference's FP32 arithmetic; its probes can then
