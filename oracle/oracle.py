@@ -37,7 +37,7 @@ def build(force: bool = False) -> None:
     tree is present (make decides from the sources' timestamps)."""
     if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < os.path.getmtime(
             os.path.join(HERE, "falconnpp_oracle.cpp")):
-        subprocess.run(["make", "-C", HERE, "-B" if force else "-s", "_build/liboracle.so" if not force else "all",
+        subprocess.run(["make", "-C", HERE, "-B" if force else "-s", LIB if not force else "all",
                         *_make_args()], check=True, capture_output=True)
     subprocess.run(["make", "-C", HERE, "-s", "ref", *_make_args()], check=True, capture_output=True)
 
