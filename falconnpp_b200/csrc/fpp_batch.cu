@@ -352,9 +352,24 @@ int batch_query(const Params& P, DeviceIndex& di, BatchWorkspace& bw, const Batc
         return fail(e, "memset");
       cudaEventRecord(bw.tev[0], s);
     }
-    // host queries: four chunks copied on the copy stream, each hashed as
-    // soon as it lands
-    const int nch = (rq.Q_host && rq.copy_stream && rq.copy_stream != s && rq.nq >= 4096) ? 4 : 1;
+    // host queries: up to four chunks copied on the copy stream, each hashed
+    // as soon as it lands.  The hash launches of one stream run one after
+    // the other, so a chunk that is not a whole number of waves of hash
+    // blocks leaves SMs idle at its end: with the verified hash the first
+    // chunks are one full wave each and the last takes the rest (the same
+    // number of waves as one launch over the batch); otherwise quarters.
+    long long cut[5] = {0, 0, 0, 0, 0};
+    int nch = (rq.Q_host && rq.copy_stream && rq.copy_stream != s && rq.nq >= 4096) ? 4 : 1;
+    if (nch > 1) {
+      const long long wq = vhash ? hash_verified_wave_queries() : 0;
+      if (wq > 0) nch = (int)std::min<long long>(4, rq.nq / wq);
+      for (int c = 0; c <= nch; ++c) cut[c] = wq > 0 ? (c < nch ? c * wq : rq.nq) : (long long)rq.nq * c / nch;
+    }
+    if (nch <= 1) {
+      nch = 1;
+      cut[0] = 0;
+      cut[1] = rq.nq;
+    }
     if (rq.Q_host && nch == 1 &&
         (e = cudaMemcpyAsync(const_cast<float*>(rq.Q), rq.Q_host, sizeof(float) * (size_t)rq.nq * d,
                              cudaMemcpyHostToDevice, s)) != cudaSuccess)
@@ -368,7 +383,7 @@ int batch_query(const Params& P, DeviceIndex& di, BatchWorkspace& bw, const Batc
       cudaEventRecord(bw.cev[4], s);
       cudaStreamWaitEvent(rq.copy_stream, bw.cev[4], 0);
       for (int c = 0; c < nch; ++c) {
-        const long long q0 = (long long)rq.nq * c / nch, q1 = (long long)rq.nq * (c + 1) / nch;
+        const long long q0 = cut[c], q1 = cut[c + 1];
         if ((e = cudaMemcpyAsync(const_cast<float*>(rq.Q) + q0 * d, rq.Q_host + q0 * d,
                                  sizeof(float) * (size_t)(q1 - q0) * d, cudaMemcpyHostToDevice, rq.copy_stream)) !=
             cudaSuccess)
@@ -377,7 +392,7 @@ int batch_query(const Params& P, DeviceIndex& di, BatchWorkspace& bw, const Batc
       }
     }
     for (int c = 0; c < nch; ++c) {
-      const long long q0 = (long long)rq.nq * c / nch, q1 = (long long)rq.nq * (c + 1) / nch;
+      const long long q0 = cut[c], q1 = cut[c + 1];
       if (nch > 1) cudaStreamWaitEvent(s, bw.cev[c], 0);
       const int* qq = rq.q_qprobes ? rq.q_qprobes + q0 : nullptr;
       e = vhash ? hash_lists_verified(P, di, rq.Q + q0 * d, (int)(q1 - q0), qq, rq.qprobes_max,

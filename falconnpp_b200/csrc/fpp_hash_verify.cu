@@ -280,6 +280,15 @@ __global__ void __launch_bounds__(kVWarps * 32) k_query_hash_verified(VerifyArgs
 
 }  // namespace
 
+long long hash_verified_wave_queries() {
+  int dev = 0, nsm = 0, per_sm = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_query_hash_verified, kVWarps * 32, 0) != cudaSuccess)
+    return 0;
+  return (long long)nsm * per_sm * kVWarps;
+}
+
 cudaError_t hash_lists_verified(const Params& P, const DeviceIndex& di, const float* Q, int nq, const int* q_qprobes,
                                 int qp_max, float* list_v, uint32_t* list_b, long long stride, unsigned* n_exact,
                                 cudaStream_t s) {

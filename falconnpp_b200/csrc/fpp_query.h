@@ -92,6 +92,10 @@ cudaError_t hash_lists_verified(const Params& P, const DeviceIndex& di, const fl
                                 int qp_max, float* list_v, uint32_t* list_b, long long stride, unsigned* n_exact,
                                 cudaStream_t s);
 
+// Queries k_query_hash_verified takes in one full wave of its blocks on the
+// current device (SMs x resident blocks x queries per block); 0 if unknown.
+long long hash_verified_wave_queries();
+
 int query_index(const Params& P, const DeviceIndex& di, const float* Q, bool q_on_device, int nq, int k,
                 int32_t* out, bool out_on_device, QueryWorkspace& ws, QueryStats& st, cudaStream_t s,
                 Error& err, QueryDumps* dumps);

@@ -183,20 +183,23 @@ def test_hash_set_overflow_falls_back_to_bitset(precision):
 @pytest.mark.parametrize("precision", [0, 1, 2])
 def test_host_queries_equal_device_queries(precision):
     # fpp_query with host buffers copies large batches in chunks that overlap
-    # the hash kernel; the results must be the device-pointer path's
+    # the hash kernel (whole waves of hash blocks, the last chunk the rest:
+    # two chunks for 6,001 queries, four for 10,007 on a B200); the results
+    # must be the device-pointer path's
     import torch
     X = synth.mixture(50_000, 200, n_centres=32, seed=0)
-    Q = synth.mixture(6001, 200, n_centres=32, seed=1)
     g = _index(X, 16, 256, 100, 0.01, 3)
     g.set_qprobes(6)
     g.set_query_form(1, precision, 2)
-    for graph in (0, 1):
-        g.set_option("use_graph", graph)
-        host = g.query(Q, 10)
-        dq = torch.from_numpy(Q).cuda()
-        out = torch.zeros((len(Q), 10), dtype=torch.int32, device="cuda")
-        g.query_device(dq.data_ptr(), len(Q), 10, out.data_ptr())
-        torch.cuda.synchronize()
-        assert np.array_equal(host, out.cpu().numpy())
-        assert np.array_equal(host, g.query(Q, 10))  # the query buffer is reused safely
+    for nq in (6001, 10007):
+        Q = synth.mixture(nq, 200, n_centres=32, seed=1)
+        for graph in (0, 1):
+            g.set_option("use_graph", graph)
+            host = g.query(Q, 10)
+            dq = torch.from_numpy(Q).cuda()
+            out = torch.zeros((len(Q), 10), dtype=torch.int32, device="cuda")
+            g.query_device(dq.data_ptr(), len(Q), 10, out.data_ptr())
+            torch.cuda.synchronize()
+            assert np.array_equal(host, out.cpu().numpy())
+            assert np.array_equal(host, g.query(Q, 10))  # the query buffer is reused safely
     g.close()
