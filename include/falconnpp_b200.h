@@ -169,10 +169,12 @@ int fpp_query_dump(fpp_index* h, const float* queries, int n_queries, int n_neig
  * top-k) with dynamic scheduling; precision 0 reranks in FP32 and equals the
  * plain path bit for bit; precision 1 (BF16) and 2 (FP8-E4M3 with a per-row
  * scale) rerank the candidates in low precision with FP32 accumulation and
- * re-score the best shortlist_mult * k of them in exact FP32.  The hashing is
- * the reference's FP32 arithmetic in every form (unless the opt-in
- * "tc_rotation" option is set), so every form probes the same buckets and
- * gathers the same candidates; only the low-precision rerank differs.
+ * re-score the best shortlist_mult * k of them in exact FP32.  Every form
+ * gets the probes of the reference's FP32 hash (the batched form's
+ * tensor-core rotation under "tc_hash" re-hashes in FP32 every table that can
+ * reach the probe cut; only the opt-in "tc_rotation" option departs from
+ * it), so every form probes the same buckets and gathers the same
+ * candidates; only the low-precision rerank differs.
  * Extends query2Layers_1D; no reference counterpart for the batched form. */
 int fpp_set_query_form(fpp_index* h, int form, int precision, int shortlist_mult);
 
