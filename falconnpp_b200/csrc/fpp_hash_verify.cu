@@ -3,7 +3,8 @@
 // decide a probe (k_query_hash_verified).  fhtDim 256, one probe per table
 // (2 qProbes <= L).
 //
-// One warp per query:
+// One block of two warps per query (the warps split the tables, and block
+// barriers join them; half-query work units keep the last wave short):
 //   1. every table's two layers rotate on the tensor cores (tc_rotate_top1:
 //      FP16 operands, FP32 accumulation) with the query scaled by a power of
 //      two; each table gets an approximate score s~ = v1~ + v2~ and code;
@@ -14,7 +15,7 @@
 //      tie with a probe;
 //   3. the other tables (usually a handful) are hashed again in the
 //      reference's FP32 arithmetic (the plain path's hd3_rotate and strict
-//      top-1, four groups of 8 lanes), and their exact scores and codes
+//      top-1, eight groups of 8 lanes), and their exact scores and codes
 //      replace the approximate ones;
 //   4. when those exact scores tie at the cut, or an approximate score is not
 //      finite, every table of the query is hashed exactly, so the probe cut's
@@ -54,10 +55,11 @@
 namespace fpp {
 namespace {
 
-constexpr int kVWarps = 4;          // queries per block (one per warp)
+constexpr int kVWarps = 2;          // warps per block; one block per query
+constexpr int kVThreads = kVWarps * 32;
 constexpr int kVMaxL = 128;         // tables per query
 constexpr int kVFht = 256;
-constexpr int kVGroups = 4;         // 8-lane groups per warp for the exact hash
+constexpr int kVGroups = 4 * kVWarps;  // 8-lane groups per block for the exact hash
 
 // relative error per layer (of ||y||) and absolute error per layer (scaled
 // units), before the factor 2 x 2
@@ -80,15 +82,15 @@ struct VerifyArgs {
 };
 
 struct VerifySmem {
-  float qs[kVWarps][kVFht];               // the query, zero padded past d
-  float sv[kVWarps][kVMaxL];              // per table: score (approximate or exact)
-  uint32_t sb[kVWarps][kVMaxL];           // per table: global bucket id
-  int rl[kVWarps][kVMaxL];                // tables to hash exactly
-  float ydump[kVWarps][kVGroups][kVFht];  // exact path: the dump a tie replays
-  float lv[kVWarps][kVGroups][2];         // exact path: per group, per layer
-  int lc[kVWarps][kVGroups][2];
-  float hv[kVWarps][kVGroups];            // replay heap (one entry)
-  int hi[kVWarps][kVGroups];
+  float qs[kVFht];               // the query, zero padded past d
+  float sv[kVMaxL];              // per table: score (approximate or exact)
+  uint32_t sb[kVMaxL];           // per table: global bucket id
+  int rl[kVMaxL];                // tables to hash exactly
+  float ydump[kVGroups][kVFht];  // exact path: the dump a tie replays
+  float lv[kVGroups][2];         // exact path: per group, per layer
+  int lc[kVGroups][2];
+  float hv[kVGroups];            // replay heap (one entry)
+  int hi[kVGroups];
 };
 
 // A non-negative score as an ordered key: its bits without the sign (a -0
@@ -118,26 +120,29 @@ __device__ __forceinline__ uint32_t warp_pth_largest(const float* v, int n, int 
 }
 
 // Hash exactly, in the plain path's arithmetic, the tables whose bit is set
-// in mask[0..4) (table lane + 32 j <-> bit lane of mask[j]); four tables at a
-// time, one per 8-lane group, both layers.  Writes their exact scores and
-// bucket ids into sv / sb (FalconnPP.cpp:358-485 for one probe per table).
+// in mask[0..4) (table lane + 32 j <-> bit lane of mask[j]; the same mask in
+// both warps); eight tables at a time, one per 8-lane group of the block,
+// both layers.  Writes their exact scores and bucket ids into sv / sb
+// (FalconnPP.cpp:358-485 for one probe per table).  Called by the whole
+// block: it starts and ends with a block barrier.
 __device__ __forceinline__ void exact_tables(const VerifyArgs& a, VerifySmem& sm, int warp, int lane,
                                              const uint32_t (&mask)[4]) {
-  int* rl = sm.rl[warp];
+  int* rl = sm.rl;
   int base = 0;
 #pragma unroll
   for (int j = 0; j < 4; ++j) {
-    if ((mask[j] >> lane) & 1u) rl[base + __popc(mask[j] & ((1u << lane) - 1u))] = lane + 32 * j;
+    if (warp == 0 && ((mask[j] >> lane) & 1u)) rl[base + __popc(mask[j] & ((1u << lane) - 1u))] = lane + 32 * j;
     base += __popc(mask[j]);
   }
-  __syncwarp();
+  __syncthreads();
   const int nr = base;
-  const int grp = lane >> 3, gl = lane & 7;
+  const int gw = lane >> 3, gl = lane & 7;
+  const int grp = warp * 4 + gw;
   const unsigned gmask = 0xffu << (lane & ~7);
   float xr[32];
 #pragma unroll
-  for (int e = 0; e < 32; ++e) xr[e] = sm.qs[warp][gl * 32 + e];
-  for (int r0 = 0; r0 < nr; r0 += kVGroups) {
+  for (int e = 0; e < 32; ++e) xr[e] = sm.qs[gl * 32 + e];
+  for (int r0 = 0; r0 < nr; r0 += kVGroups) {  // uniform over the block
     const bool act = r0 + grp < nr;
     const int l = rl[act ? r0 + grp : r0];
 #pragma unroll 1
@@ -146,47 +151,47 @@ __device__ __forceinline__ void exact_tables(const VerifyArgs& a, VerifySmem& sm
 #pragma unroll
       for (int e = 0; e < 32; ++e) y[e] = xr[e];
       hd3_rotate<kVFht>(y, a.flips + ((size_t)(layer * a.L + l) * 3) * 8, gl);
-      float* ov = &sm.lv[warp][grp][layer];
-      int* oc = &sm.lc[warp][grp][layer];
+      float* ov = &sm.lv[grp][layer];
+      int* oc = &sm.lc[grp][layer];
       const bool ok = group_top1_strict<kVFht>(y, gl, a.D, a.log2D, ov, oc);
       __syncwarp();
       if (!ok) {
         // a tie for the best coordinate (or D < 2): the reference's scan
-        float* yd = sm.ydump[warp][grp];
+        float* yd = sm.ydump[grp];
 #pragma unroll
         for (int e = 0; e < 32; ++e) yd[gl * 32 + e] = y[e];
         __syncwarp(gmask);
-        if (gl == 0) replay_layer_topp(yd, a.D, a.log2D, 1, &sm.hv[warp][grp], &sm.hi[warp][grp], ov, oc);
+        if (gl == 0) replay_layer_topp(yd, a.D, a.log2D, 1, &sm.hv[grp], &sm.hi[grp], ov, oc);
         __syncwarp(gmask);
       }
     }
     __syncwarp();
     if (gl == 0 && act) {
-      sm.sv[warp][l] = __fadd_rn(sm.lv[warp][grp][0], sm.lv[warp][grp][1]);
-      sm.sb[warp][l] = (uint32_t)l * a.NB + (uint32_t)(sm.lc[warp][grp][0] * 2 * a.D + sm.lc[warp][grp][1]);
+      sm.sv[l] = __fadd_rn(sm.lv[grp][0], sm.lv[grp][1]);
+      sm.sb[l] = (uint32_t)l * a.NB + (uint32_t)(sm.lc[grp][0] * 2 * a.D + sm.lc[grp][1]);
     }
     __syncwarp();
   }
+  __syncthreads();
 }
 
-__global__ void __launch_bounds__(kVWarps * 32) k_query_hash_verified(VerifyArgs a) {
+// Every branch below that contains a block barrier depends only on values
+// both warps compute alike from shared memory (the norm, the scores, the
+// masks), so both warps take it.
+__global__ void __launch_bounds__(kVThreads, 8) k_query_hash_verified(VerifyArgs a) {
   __shared__ VerifySmem sm;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int q = blockIdx.x * kVWarps + warp;
-  if (q >= a.nq) return;  // warp-uniform; the block never synchronises
+  const int q = blockIdx.x;  // one query per block
   const int L = a.L;
-  float* qs = sm.qs[warp];
-  float* sv = sm.sv[warp];
-  uint32_t* sb = sm.sb[warp];
-  float ss = 0.0f;
-  for (int i = lane; i < kVFht; i += 32) {
-    const float x = i < a.d ? __ldg(a.Q + (size_t)q * a.d + i) : 0.0f;
-    qs[i] = x;
-    ss = fmaf(x, x, ss);
-  }
+  float* qs = sm.qs;
+  float* sv = sm.sv;
+  uint32_t* sb = sm.sb;
+  for (int i = threadIdx.x; i < kVFht; i += kVThreads) qs[i] = i < a.d ? __ldg(a.Q + (size_t)q * a.d + i) : 0.0f;
+  __syncthreads();
+  float ss = 0.0f;  // the same sum, in the same order, in both warps
+  for (int i = lane; i < kVFht; i += 32) ss = fmaf(qs[i], qs[i], ss);
 #pragma unroll
   for (int o = 16; o; o >>= 1) ss += __shfl_xor_sync(kFullMask, ss, o);
-  __syncwarp();
   const float nrm = sqrtf(ss);
   // far from FP32's range limits (and finite), the bound holds; otherwise
   // every table is hashed exactly
@@ -207,7 +212,8 @@ __global__ void __launch_bounds__(kVWarps * 32) k_query_hash_verified(VerifyArgs
     const H16Frags hf(lane);
     uint32_t qb[2][2];
     tc_query_frags(qs, scale, lane, qb);
-    for (int l = 0; l < L; l += 2) {
+    // the warps take alternate pairs of tables
+    for (int l = 2 * warp; l < L; l += 2 * kVWarps) {
       const int l2 = l + 1 < L ? l + 1 : l;
       const uint32_t* const tw[4] = {a.tflips + (size_t)l * 24, a.tflips + (size_t)(L + l) * 24,
                                      a.tflips + (size_t)l2 * 24, a.tflips + (size_t)(L + l2) * 24};
@@ -223,7 +229,7 @@ __global__ void __launch_bounds__(kVWarps * 32) k_query_hash_verified(VerifyArgs
         }
       }
     }
-    __syncwarp();
+    __syncthreads();
     // delta per table in the query's own units; the norm rounded up
     const float ny = nrm * (1.0f + 0x1p-12f) * 4096.0f;
     const float delta = 4.0f * (kVRelLayer * ny + kVAbsLayer * inv);
@@ -260,7 +266,7 @@ __global__ void __launch_bounds__(kVWarps * 32) k_query_hash_verified(VerifyArgs
       all = true;
     }
   }
-  if (a.n_exact && lane == 0) {
+  if (a.n_exact && threadIdx.x == 0) {
     unsigned n = 0;
     if (all) {
       n = (unsigned)L;
@@ -272,7 +278,7 @@ __global__ void __launch_bounds__(kVWarps * 32) k_query_hash_verified(VerifyArgs
   }
   float* ov = a.list_v + (size_t)q * a.stride;
   uint32_t* ob = a.list_b + (size_t)q * a.stride;
-  for (int i = lane; i < L; i += 32) {
+  for (int i = threadIdx.x; i < L; i += kVThreads) {
     ov[i] = sv[i];
     ob[i] = sb[i];
   }
@@ -284,9 +290,9 @@ long long hash_verified_wave_queries() {
   int dev = 0, nsm = 0, per_sm = 0;
   if (cudaGetDevice(&dev) != cudaSuccess ||
       cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_query_hash_verified, kVWarps * 32, 0) != cudaSuccess)
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_query_hash_verified, kVThreads, 0) != cudaSuccess)
     return 0;
-  return (long long)nsm * per_sm * kVWarps;
+  return (long long)nsm * per_sm;  // one query per block
 }
 
 cudaError_t hash_lists_verified(const Params& P, const DeviceIndex& di, const float* Q, int nq, const int* q_qprobes,
@@ -314,7 +320,7 @@ cudaError_t hash_lists_verified(const Params& P, const DeviceIndex& di, const fl
   a.list_b = list_b;
   a.stride = stride;
   a.n_exact = n_exact;
-  k_query_hash_verified<<<(unsigned)((nq + kVWarps - 1) / kVWarps), kVWarps * 32, 0, s>>>(a);
+  k_query_hash_verified<<<(unsigned)nq, kVThreads, 0, s>>>(a);
   return cudaGetLastError();
 }
 

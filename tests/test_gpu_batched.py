@@ -184,8 +184,8 @@ def test_hash_set_overflow_falls_back_to_bitset(precision):
 def test_host_queries_equal_device_queries(precision):
     # fpp_query with host buffers copies large batches in chunks that overlap
     # the hash kernel (whole waves of hash blocks, the last chunk the rest:
-    # two chunks for 6,001 queries, four for 10,007 on a B200); the results
-    # must be the device-pointer path's
+    # several chunks for these batch sizes on a B200); the results must be
+    # the device-pointer path's
     import torch
     X = synth.mixture(50_000, 200, n_centres=32, seed=0)
     g = _index(X, 16, 256, 100, 0.01, 3)
