@@ -545,13 +545,13 @@ int fpp_autotune(fpp_index* h, const float* d_queries, int n_queries, int k, dou
     best_ms = ms;
     best_agree = 1.0;
     const int precs[2] = {1, 2};
-    const int mults[3] = {1, 2, 4};
+    const int mults[2] = {2, 4};  // the exact FP32 re-score of a 2-4 x k shortlist
     const int bpss[3] = {1, 2, 3};
     // precision x shortlist x resident blocks per SM (queries in flight per
     // SM) x exact hash in its own kernel or inside the fused one x query
     // grouping; the hash and grouping choices change no result
     for (int pi = 0; pi < 2 && rc == FPP_OK; ++pi)
-      for (int mi = 0; mi < 3 && rc == FPP_OK; ++mi)
+      for (int mi = 0; mi < 2 && rc == FPP_OK; ++mi)
         for (int bi = 0; bi < 3 && rc == FPP_OK; ++bi)
           for (int sp = 1; sp >= 0 && rc == FPP_OK; --sp)
             for (int ro = 1; ro >= 0 && rc == FPP_OK; --ro) {

@@ -206,7 +206,7 @@ int fpp_query_batched_dump(fpp_index* h, const float* d_queries, int n_queries, 
 
 /* Autotuner of the batched form (no reference counterpart).  On a sample of
  * device queries it times the batched form over precision {BF16, FP8} x
- * shortlist multiple {1,2,4} x resident fused blocks per SM {1,2,3} (each
+ * shortlist multiple {2,4} x resident fused blocks per SM {1,2,3} (each
  * block works on one query at a time, so this is the queries in flight per
  * SM) x exact hash in its own kernel or inside the fused one x query grouping
  * on/off, against the FP32 exact batched result, and keeps the fastest
